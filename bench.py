@@ -1,0 +1,346 @@
+#!/usr/bin/env python3
+"""Benchmark of the multislice raster: probe*slice propagations per second.
+
+Workload (the configuration the headline metric is quoted on): FEM variance
+of one amorphous-Si specimen, ~50,000 atoms at seeded random positions with
+a 2.2 A minimum separation in a 100 A cube, 1024x1024 grid, 2 A minimum slice
+thickness (~50 slices), 200 kV, 1.5 mrad probe aperture, 64x64 probe raster,
+V_omega and V_re over 200 k bins (--dr 1.2065).  Synthetic, seeded inputs
+stand in for real specimens.
+
+One step = one whole raster (4,096 probes through every slice, detection and
+FEM statistics) on a device-resident specimen; `value` is whole-job
+throughput over all ranks.  `e2e` is the same metric through the C ABI from
+host buffers: each step uploads the atoms, builds the specimen on the device
+(LUTs, slicing, transmission functions), runs the raster and copies the
+results back.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank runs its own replica of the job on its GPU (the
+probes are independent; there is no data-path collective), so scaling is
+weak; rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "ms-stem-fem_b200"))
+
+METRIC = "probe*slice props/s @1024^2 (FEM V(k), batched FP32 wavefields)"
+UNIT = "probe*slices/s"
+WORKLOAD = dict(n_atoms=50000, box=(100.0, 100.0, 100.0), seed=2,
+                argv=("-m 1024 1024 200000 --adfstemuncorrfem --V_omega --V_re --cs3 1.3e7 "
+                      "--defocus 0 --alphamax 0.0015 --rasterspacing 1.5625 --minslice 2.0 "
+                      "--dr 1.2065"))
+
+
+def make_specimen(path):
+    import specimen
+    specimen.make_specimen(path, WORKLOAD["n_atoms"], WORKLOAD["box"], seed=WORKLOAD["seed"])
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name="row_col_pass_1024_fp32.md"):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/), or None before one was captured."""
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="msf_clocks", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def reference_sample(n_procs, cap_seconds=240):
+    """The reference's own CPU code (oracle/_ref, FFTW replaced by the oracle
+    shim's FP64 FFT) on a bounded sample of the workload: the same 1024^2
+    grid, optics and 1.5625 A raster spacing on a 100x100x6 A slab of the
+    specimen (3 slices) and 4 probes, one process per host core.  Returns
+    aggregate probe*slices/s over the cores and the sample description."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    import specimen
+    if not oracle.ref_available():
+        return None
+    work = Path(tempfile.mkdtemp(prefix="msf_refbench"))
+    rng_pos = specimen.amorphous_positions(3000, (100.0, 100.0, 6.0), seed=21)
+    rng_pos = np.round(rng_pos, 6)
+    specimen.write_lammps_data(work / "slab.data", rng_pos, (100.0, 100.0, 6.0))
+    argv = ["-a", "slab.data", "--output_prefix", "s"] + WORKLOAD["argv"].split()
+    argv[argv.index("--rasterspacing") + 1] = "50"
+    procs = []
+    t0 = time.time()
+    for k in range(n_procs):
+        d = work / ("p%d" % k)
+        d.mkdir()
+        os.link(work / "slab.data", d / "slab.data")
+        procs.append(subprocess.Popen([str(oracle.REF_BIN)] + argv, cwd=d,
+                                      stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                                      text=True))
+    total_ps, worst = 0, 0.0
+    for p in procs:
+        try:
+            _, err = p.communicate(timeout=cap_seconds)
+        except subprocess.TimeoutExpired:
+            p.kill()
+            continue
+        for line in err.splitlines():
+            if "adfstem_seconds=" in line:
+                kv = dict(x.split("=") for x in line.split()[1:])
+                total_ps += int(kv["probes"]) * int(kv["slices"])
+                worst = max(worst, float(kv["adfstem_seconds"]))
+    wall = time.time() - t0
+    if not worst:
+        return None
+    return {"value": total_ps / worst, "cores": n_procs,
+            "sample": "%d processes x (4 probes x 3 slices at 1024^2, 100x100x6 A slab, "
+                      "3000 Si); raster time only; FFT = oracle shim FP64 radix-2 (FFTW "
+                      "absent)" % n_procs, "wall_s": round(wall, 1)}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    vals = []
+    sample = None
+    for _ in range(max(1, args.steps)):  # no warm-up: nothing to compile or cache
+        s = reference_sample(cores, cap_seconds=300)
+        if s is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/ms-stem-fem-ref was not built (needs the "
+                              "reference sources at build time)"}))
+            return 0
+        vals.append(s["value"])
+        sample = s
+        if len(vals) >= max(1, args.steps):
+            break
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": len(vals), "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "FEM 1024^2 amorphous Si (bounded CPU sample)",
+                       "grid": 1024, "raster": "2x2", "slices": 3},
+            "cpu_baseline": {"kind": "reference", "cores": sample["cores"],
+                             "sample": sample["sample"], "value": v, "unit": UNIT},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="msf", choices=["msf", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import msf
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    work = Path(tempfile.mkdtemp(prefix="msf_bench_r%d_" % rank))
+    spec_path = work / "c2.data"
+    make_specimen(spec_path)
+    argv = ["-a", str(spec_path), "--output_prefix", str(work / "c2")] + WORKLOAD["argv"].split()
+    job = msf.Job(argv)
+    q, z = job.positions()
+    ctx = msf.Context(device=local, precision=args.precision, batch=args.batch,
+                      graphs=not args.no_graphs)
+    t0 = time.time()
+    spec = ctx.specimen(job.grid, q, z)
+    setup_s = time.time() - t0
+    n_slices = spec.slices()["n"]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ctx.run(spec, job.optics, job.raster, job.detect)
+    barrier()
+    dev_times, launches, ps = [], 0, 0
+    with ClockSampler(local) as clocks:
+        wall0 = time.time()
+        for _ in range(args.steps):
+            r = ctx.run(spec, job.optics, job.raster, job.detect)
+            dev_times.append(r.seconds_raster)
+            launches += r.kernel_launches
+            ps += r.probe_slices
+        wall = time.time() - wall0
+    barrier()
+    total_dev = sum(dev_times)
+    if dist is not None:
+        import torch
+        t = torch.tensor([total_dev], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_dev = float(t.item())
+    value = ps * world / total_dev
+    ms_per_step = 1e3 * total_dev / args.steps
+
+    # roofline of the dominant kernel (fused row / column slice pass)
+    nb = max(1, min(32, job.n_probes))
+    ms_row, ms_col = ctx.time_passes(spec, nb, reps=20)
+    n = job.grid.nx
+    cbytes = 8 if args.precision == "fp32" else 16
+    alg = 2.0 * n * n * cbytes * nb  # read + write of nb wavefields per pass
+    dom = "col" if ms_col >= ms_row else "row"
+    t_dom = max(ms_row, ms_col) * 1e-3
+    peak, peak_kind = measured_peaks()
+    achieved = alg / t_dom / 1e9
+    traffic = ncu_traffic()
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "%s pass (fused FFT + %s), %d probes/launch" %
+                          (dom, "transmission" if dom == "row" else "propagator", nb),
+                "peak_source": peak_kind, "ms_row": round(ms_row, 4), "ms_col": round(ms_col, 4),
+                "algorithmic_bytes_per_launch": alg}
+
+    # end to end through the C ABI from host buffers
+    e2e = None
+    if not args.no_e2e:
+        ctx.transfer_bytes(reset=True)
+        t0 = time.time()
+        e2e_steps = max(1, min(2, args.steps))
+        e2e_ps = 0
+        for _ in range(e2e_steps):
+            s2 = ctx.specimen(job.grid, q, z)
+            r2 = ctx.run(s2, job.optics, job.raster, job.detect)
+            e2e_ps += r2.probe_slices
+            s2.close()
+        e2e_t = time.time() - t0
+        h2d, d2h = ctx.transfer_bytes(reset=True)
+        h2d += q.nbytes + z.nbytes  # atoms staged into the specimen build
+        e2e = {"value": e2e_ps * world / e2e_t if world == 1 else None, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d / e2e_steps),
+               "d2h_bytes_per_step": int(d2h / e2e_steps),
+               "includes": "atom upload, LUT/slicing/transmission build, raster, result copy"}
+        if dist is not None:
+            import torch
+            t = torch.tensor([e2e_t], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e["value"] = e2e_ps * world / float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        s = reference_sample(os.cpu_count() or 1)
+        if s is not None:
+            cpu = {"value": s["value"], "unit": UNIT, "cores": s["cores"], "kind": "reference",
+                   "sample": s["sample"]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 2),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+                "config": {"workload": "FEM V(k) single specimen: 50k Si, 100 A cube, 1024^2, "
+                                       "64x64 raster, %d slices" % n_slices,
+                           "probes": job.n_probes, "slices": n_slices,
+                           "probe_slices_per_step": ps // args.steps,
+                           "parallelism": "replica per GPU (probes independent)",
+                           "l2": "inputs exceed L2: %.0f MB of transmission functions" %
+                                 (spec.device_bytes() / 1e6),
+                           "graphs": not args.no_graphs, "batch": args.batch or "auto",
+                           "specimen_setup_s": round(setup_s, 3)},
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clocks.summary(), "gpu_launches": int(launches),
+                "wall_s_timed": round(wall, 3)}
+        print(json.dumps(line))
+    spec.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,232 @@
+/* msf.h -- C ABI of the B200 multislice ADF-STEM / FEM library (libmsf.so).
+ *
+ * Plain C: opaque handles, POD structs, caller-owned host buffers, integer
+ * status codes (never exit()).  One CUDA stream per context; contexts are
+ * independent, so separate threads may drive separate contexts.
+ *
+ * The reference (nickjulian/ms-stem-fem) is one MPI executable with no FFI;
+ * these entry points replace its multislice path at the function boundary:
+ *
+ *   msf_specimen_create   replaces tem.cpp:944-1276 -- scatterer_pap_LUT
+ *                         (scatterer_pap.hpp:45-230), assign_atoms_to_slices_
+ *                         z_auto (slice.cpp:469-980), slice::update_propagator
+ *                         (slice.cpp:1293-1363) and slice::update_transmission_
+ *                         function (slice.cpp:1451-1757)
+ *   msf_run               replaces TEM_NS::adfstem (adfstem.hpp:66-122,
+ *                         adfstem.cpp:37-4096): probe, raster, slice loop,
+ *                         ADF detection and the FEM V(k) statistics
+ *   msf_parse_cmdline     replaces read_cmdline_options / read_parameter_file
+ *                         / check_runtime_flags (tem_io.cpp:5277-5720,
+ *                         4063-4626, 5858-6169) plus tem.cpp's defaults
+ *   msf_read_specimen     replaces read_position_lammps_data_file
+ *                         (tem_io.cpp:36-1028) and read_position_xyz_file
+ *                         (tem_io.cpp:4627-4958)
+ *   msf_write_outputs     replaces output_variance_to_txt (io_txt.cpp:30-94)
+ *                         and output_stem_image (write_tif.cpp:1552-1605)
+ */
+#ifndef MSF_H
+#define MSF_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSF_ABI_VERSION 1
+
+typedef enum {
+  MSF_OK = 0,
+  MSF_ERR_ARG = 1,         /* invalid argument or inconsistent request     */
+  MSF_ERR_UNSUPPORTED = 2, /* valid for the reference, not built here      */
+  MSF_ERR_CUDA = 3,        /* CUDA runtime error (message via msf_last_error) */
+  MSF_ERR_NOMEM = 4,       /* device or host allocation failed             */
+  MSF_ERR_IO = 5,          /* file could not be read or written            */
+  MSF_ERR_PARSE = 6,       /* malformed command line / parameter / specimen */
+  MSF_ERR_TIMEOUT = 7,     /* a bounded device wait gave up                */
+  MSF_ERR_BUSY = 8,        /* serving queue full / budget exhausted        */
+  MSF_ERR_CANCELLED = 9
+} msf_status;
+
+typedef enum { MSF_FP64 = 0, MSF_FP32 = 1 } msf_precision;
+
+/* FEM modes (tem_io.cpp:5563-5586) and image output, as bits. */
+#define MSF_OUT_ADF_IMAGE    (1u << 0) /* --images                          */
+#define MSF_OUT_V_OMEGA      (1u << 1) /* --V_omega     (flags.d1)          */
+#define MSF_OUT_VBAR_R       (1u << 2) /* --Vbar_r      (flags.d2)          */
+#define MSF_OUT_V_RE         (1u << 3) /* --V_re        (flags.d3)          */
+#define MSF_OUT_OMEGA_VIMAGE (1u << 4) /* --Omega_vimage (flags.d4)         */
+#define MSF_OUT_V_GT17       (1u << 5) /* --V_gt17      (flags.gt17)        */
+#define MSF_OUT_V_RBAR       (1u << 6) /* --V_rbar      (flags.rva)         */
+#define MSF_OUT_FEM_MASK     (0x7eu)
+
+typedef struct msf_context msf_context;
+typedef struct msf_specimen msf_specimen;
+
+typedef struct {
+  int32_t device;          /* CUDA device ordinal                              */
+  int32_t precision;       /* msf_precision of wavefields and FFTs             */
+  int32_t batch;           /* probes per launch; 0 = choose from free memory   */
+  int32_t use_graphs;      /* capture each batch's slice stack in a CUDA graph */
+  int64_t hbm_budget;      /* bytes this context may allocate; 0 = no limit    */
+} msf_options;
+
+/* Simulation cell and grid (tem.cpp:405-695). */
+typedef struct {
+  int32_t nx, ny;          /* -m samples_x samples_y                           */
+  double voltage;          /* -m VV [V]                                        */
+  double xperiod, yperiod, zperiod; /* specimen periods [A] (raster uses x,y)  */
+  int32_t dupe_x, dupe_y, dupe_z;   /* --dupe period multipliers (1 1 1 if absent) */
+  int32_t replicate_atoms;  /* 1: copy the atoms into every duped cell, as
+                               tem.cpp:1051-1143 does for FEM runs only      */
+  double xmin, ymin, zmin; /* domain origin (0 after the LAMMPS reader shift)  */
+  double min_slice;        /* --minslice [A]                                   */
+} msf_grid;
+
+typedef struct {
+  int64_t n_atoms;
+  const double* q;         /* 3*n_atoms: x y z [A] per atom                    */
+  const uint32_t* z;       /* atomic numbers 1..103                            */
+} msf_atoms;
+
+typedef struct {
+  int32_t corrected;       /* 0: uncorrected chi, 1: Cs5-corrected chi         */
+  double cs3, cs5;         /* [A]                                              */
+  double defocus;          /* [A]                                              */
+  double alpha_max;        /* probe-forming aperture [rad]                     */
+} msf_optics;
+
+typedef struct {
+  int32_t n_x, n_y;        /* raster points                                    */
+  const double* x_p;       /* n_x positions [A]                                */
+  const double* y_p;       /* n_y positions [A]                                */
+} msf_raster;
+
+typedef struct {
+  uint32_t outputs;        /* MSF_OUT_* bits                                   */
+  double det_inner, det_outer; /* ADF detector angles [rad]                    */
+  double dr;               /* --dr azimuthal_binning_size_factor               */
+} msf_detect;
+
+/* Caller-owned result buffers; any pointer may be NULL when not wanted. */
+typedef struct {
+  double* adf_image;       /* n_x*n_y, row px, column py: [px*n_y + py]        */
+  int32_t cap_k;           /* capacity of each per-bin array below            */
+  int32_t n_k;             /* out: number of k bins                            */
+  double* k_lower;         /* out: lower boundary of each bin [1/A]            */
+  int32_t* bin_counts;     /* out: pixels per bin                              */
+  double* v_omega;
+  double* vbar_r;
+  double* v_re;
+  double* omega_vimage;
+  double* v_gt17;
+  double* v_rbar;
+  double* final_psi;       /* 2*nx*ny: last probe's exit wave in k-space      */
+  double* mean_amplitude;  /* nx*ny: raster mean of |psi(k)| (FEM pixel modes)*/
+  double* mean_intensity;  /* nx*ny: raster mean of |psi(k)|^2                */
+  int64_t probe_slices;    /* out: probe*slice propagations performed          */
+  int64_t kernel_launches; /* out: CUDA kernels this call launched (incl. the
+                              kernels inside replayed graphs)                 */
+  double seconds_setup;    /* out: specimen set-up time (msf_run: 0)           */
+  double seconds_raster;   /* out: device time of the raster                   */
+} msf_results;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t msf_abi_version(void);
+const char* msf_last_error(void);            /* thread-local message        */
+const char* msf_status_string(msf_status s);
+
+/* ---- context ---------------------------------------------------------- */
+msf_status msf_context_create(const msf_options* opt, msf_context** out);
+msf_status msf_context_destroy(msf_context* ctx);
+msf_status msf_context_synchronize(msf_context* ctx);
+/* Host<->device bytes this context has copied since the last reset
+ * (reset != 0 zeroes the counters after reading). */
+msf_status msf_context_transfer_bytes(msf_context* ctx, int64_t* h2d,
+                                      int64_t* d2h, int32_t reset);
+
+/* ---- specimen: LUTs, slicing, propagators, transmission functions ------ */
+msf_status msf_specimen_create(msf_context* ctx, const msf_grid* grid,
+                               const msf_atoms* atoms, msf_specimen** out);
+msf_status msf_specimen_destroy(msf_specimen* spec);
+/* Slice count and per-slice lower bound, thickness and atom count (any
+ * pointer may be NULL; arrays hold `cap` entries). */
+msf_status msf_specimen_slices(const msf_specimen* spec, int32_t* n_slices,
+                               double* lower, double* thickness,
+                               int64_t* atoms_per_slice, int32_t cap);
+/* Copy one slice's transmission function t(x,y) to host, 2*nx*ny doubles
+ * interleaved re/im, row-major [x][y] as the reference's exp_i_sigma_v. */
+msf_status msf_specimen_transmission(const msf_specimen* spec, int32_t slice,
+                                     double* out);
+/* Bytes of device memory the specimen holds. */
+int64_t msf_specimen_device_bytes(const msf_specimen* spec);
+
+/* ---- the multislice raster (adfstem) ----------------------------------- */
+msf_status msf_run(msf_context* ctx, const msf_specimen* spec,
+                   const msf_optics* optics, const msf_raster* raster,
+                   const msf_detect* detect, msf_results* results);
+/* Normalised real-space probe (adfstem.cpp:586-817), 2*nx*ny doubles. */
+msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
+                     const msf_optics* optics, double* out);
+
+/* ---- host-side set-up helpers (bit-exact with the reference) ----------- */
+/* lambda [A] and gamma for an accelerating voltage (tem.cpp:424-438). */
+void msf_wavelength(double voltage, double* lambda, double* gamma);
+/* Scherzer conditions (scherzer.cpp:61-168); which: 0 defocus_uncorrected,
+ * 1 alphamax_uncorrected, 2 defocus_corrected, 3 alphamax_corrected,
+ * 4 cs3_corrected.  `aberration` is Cs3 (0,1) or Cs5 (2,3,4). */
+double msf_scherzer(int32_t which, double lambda, double aberration);
+/* Raster positions (func.cpp:108-127): n = floor(period/spacing). */
+int32_t msf_raster_points(double period, double origin, double spacing,
+                          double* out, int32_t cap);
+/* Pixel snap of each raster probe with the reference's carried-over search
+ * (adfstem.cpp:1590-1606); shifts[2*k] = sx, [2*k+1] = sy in raster order. */
+msf_status msf_probe_shifts(const msf_grid* grid, const msf_raster* raster,
+                            int64_t* shifts);
+/* Ring bin of every pixel (-1 outside all bins) and bin count for --dr. */
+msf_status msf_ring_bins(const msf_grid* grid, double dr, int32_t* bins,
+                         int32_t* n_k);
+/* Slicing alone (slice.cpp:469-980): host only.  order[n] receives atom
+ * indices in slice order; lower/thickness/counts hold up to `cap` slices. */
+msf_status msf_slice_atoms(int64_t n_atoms, const double* q, double zmin,
+                           double zperiod, double min_slice, int32_t* n_slices,
+                           double* lower, double* thickness, int64_t* counts,
+                           int64_t* order, int32_t cap);
+
+/* ---- measurement hook (no counterpart in the reference) ---------------- */
+/* Time the two fused slice passes on a resident batch of `nb` wavefields:
+ * `reps` launches of each, CUDA events on the context's stream around each
+ * launch; returns the mean milliseconds per launch of the row pass and of
+ * the column pass. */
+msf_status msf_time_passes(msf_context* ctx, const msf_specimen* spec,
+                           int32_t nb, int32_t reps, double* ms_row,
+                           double* ms_col);
+
+/* ---- drop-in front end -------------------------------------------------- */
+typedef struct msf_job msf_job;   /* parsed command line + specimen         */
+/* Parse argv exactly as ms-stem-fem does (tem.cpp:81-403): options,
+ * --parameter_file, flag checks, specimen file, defaults.  On failure the
+ * returned status is non-zero and msf_last_error() holds the message the
+ * reference would print. */
+msf_status msf_parse_cmdline(int32_t argc, const char* const* argv,
+                             msf_job** out);
+msf_status msf_job_destroy(msf_job* job);
+/* Views into a parsed job (valid until msf_job_destroy). */
+msf_status msf_job_describe(const msf_job* job, msf_grid* grid,
+                            msf_atoms* atoms, msf_optics* optics,
+                            msf_raster* raster, msf_detect* detect);
+const char* msf_job_output_prefix(const msf_job* job); /* incl. _adfstem_* */
+/* Read a LAMMPS data or .xyz specimen; the arrays are owned by the job. */
+msf_status msf_read_specimen(const char* path, msf_job** out);
+/* Write the reference's output files for a finished run: <prefix>_fem_*.txt
+ * and <prefix>_stem_image_output{,_logscale}.tif (+ raw .f64 image). */
+msf_status msf_write_outputs(const msf_job* job, const msf_results* res);
+/* The whole drop-in program: parse, build, run, write.  Returns the process
+ * exit status the reference would return (0 success, 1 failure). */
+int32_t msf_main(int32_t argc, const char* const* argv,
+                 const msf_options* opt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSF_H */

@@ -1,0 +1,671 @@
+// Device engine: specimen build and the batched multislice raster.
+//
+// Set-up (FP64 on the device): per-species projected-potential LUT
+// (scatterer_pap.hpp:45-230), per-slice transmission functions
+// (slice.cpp:1451-1757) and the probe (adfstem.cpp:586-817).  Raster:
+// probes in raster order are processed B at a time; each batch runs
+// 2 x n_slices fused FFT passes (optionally replayed from a captured CUDA
+// graph), then the detector / ring reductions.  Per-probe ring sums and ADF
+// values stay on the device until the raster ends; the FEM statistics are
+// then finished on the host in FP64 in the reference's order
+// (adfstem.cpp:2489-3612).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "kernels.h"
+
+namespace msf {
+
+namespace {
+thread_local std::string g_error;
+
+#define MSF_CUDA(call)                                                      \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) +      \
+                " at " + __FILE__ + ":" + std::to_string(__LINE__));        \
+      return MSF_ERR_CUDA;                                                  \
+    }                                                                       \
+  } while (0)
+
+#define MSF_TRY(call)                \
+  do {                               \
+    msf_status s_ = (call);          \
+    if (s_ != MSF_OK) return s_;     \
+  } while (0)
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+template <typename T>
+msf_status upload(msf_context* ctx, DevBuf* b, const std::vector<T>& h) {
+  MSF_TRY(ctx->alloc(b, std::max<size_t>(1, h.size()) * sizeof(T)));
+  if (!h.empty()) {
+    MSF_CUDA(cudaMemcpyAsync(b->p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    ctx->h2d_bytes += (int64_t)(h.size() * sizeof(T));
+  }
+  return MSF_OK;
+}
+}  // namespace
+
+void set_error(const std::string& msg) { g_error = msg; }
+const char* last_error() { return g_error.c_str(); }
+
+void DevBuf::release() {
+  if (p) {
+    cudaFree(p);
+    if (counter) *counter -= (int64_t)bytes;
+  }
+  p = nullptr;
+  bytes = 0;
+  counter = nullptr;
+}
+
+}  // namespace msf
+
+using namespace msf;
+
+msf_status msf_context::alloc(DevBuf* b, size_t bytes) {
+  b->release();
+  if (budget > 0 && allocated + (int64_t)bytes > budget) {
+    set_error("device allocation of " + std::to_string(bytes) +
+              " bytes exceeds the context's HBM budget");
+    return MSF_ERR_NOMEM;
+  }
+  cudaError_t e = cudaMalloc(&b->p, bytes);
+  if (e != cudaSuccess) {
+    b->p = nullptr;
+    set_error(std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    return MSF_ERR_NOMEM;
+  }
+  b->bytes = bytes;
+  b->counter = &allocated;
+  allocated += (int64_t)bytes;
+  return MSF_OK;
+}
+
+msf_status msf_context::twiddles(int n, bool want64, const void** out) {
+  auto& m = want64 ? tw64 : tw32;
+  auto it = m.find(n);
+  if (it == m.end()) {
+    std::vector<double> h(2 * (size_t)n);
+    fill_twiddles(n, h.data());
+    DevBuf b;
+    if (want64) {
+      MSF_TRY(upload(this, &b, h));
+    } else {
+      std::vector<float> f(h.begin(), h.end());
+      MSF_TRY(upload(this, &b, f));
+    }
+    it = m.emplace(n, std::move(b)).first;
+  }
+  *out = it->second.p;
+  return MSF_OK;
+}
+
+namespace msf {
+
+namespace {
+
+// Plain 2-D transforms of nb FP64 planes: forward (sign -1) or inverse with
+// a scale, as row pass + column pass.
+msf_status fft2d_f64(msf_context* ctx, const Grid& g, double* planes, int nb, bool inverse,
+                     double scale) {
+  PassArgs a;
+  a.psi = planes;
+  a.batch_stride = (int64_t)g.nx * g.ny;
+  a.nb = nb;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
+  a.scale = 1.0;
+  MSF_CUDA(launch_row(true, inverse ? ROW_INV : ROW_FWD, a, ctx->stream));
+  MSF_TRY(ctx->twiddles(g.nx, true, &a.tw));
+  a.scale = scale;
+  if (inverse) {
+    MSF_CUDA(launch_col(true, COL_INV, a, ctx->stream));
+  } else {
+    MSF_CUDA(launch_col(true, COL_FWD, a, ctx->stream));
+    if (scale != 1.0)
+      MSF_CUDA(launch_scale(planes, a.batch_stride * nb, scale, nullptr, ctx->stream));
+  }
+  return MSF_OK;
+}
+
+bool grid_ok(int n) { return supported_length(n); }
+
+}  // namespace
+
+msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms* atoms,
+                          msf_specimen* spec) {
+  const double t0 = now_s();
+  if (!gin || !atoms) { set_error("null grid or atoms"); return MSF_ERR_ARG; }
+  if (!grid_ok(gin->nx) || !grid_ok(gin->ny)) {
+    set_error("grid " + std::to_string(gin->nx) + "x" + std::to_string(gin->ny) +
+              " unsupported: each side must be a power of two in [64, 4096]");
+    return MSF_ERR_UNSUPPORTED;
+  }
+  if (!(gin->xperiod > 0 && gin->yperiod > 0)) { set_error("periods must be positive"); return MSF_ERR_ARG; }
+  const int dx = std::max(1, gin->dupe_x), dy = std::max(1, gin->dupe_y),
+            dz = std::max(1, gin->dupe_z);
+  // tem.cpp:1051-1143: replicate the cell when --dupe was given (FEM only;
+  // the caller passes 1 1 1 otherwise).
+  std::vector<double> q;
+  std::vector<uint32_t> zz;
+  const int64_t n0 = atoms->n_atoms;
+  if (gin->replicate_atoms && dx * dy * dz > 1) {
+    q.resize(3 * (size_t)n0 * dx * dy * dz);
+    zz.resize((size_t)n0 * dx * dy * dz);
+    for (int ii = 0; ii < dx; ++ii)
+      for (int jj = 0; jj < dy; ++jj)
+        for (int kk = 0; kk < dz; ++kk)
+          for (int64_t i = 0; i < n0; ++i) {
+            const size_t k = (size_t)(i + n0 * (kk + dz * (jj + dy * ii)));
+            q[3 * k] = atoms->q[3 * i] + ii * gin->xperiod;
+            q[3 * k + 1] = atoms->q[3 * i + 1] + jj * gin->yperiod;
+            q[3 * k + 2] = atoms->q[3 * i + 2] + kk * gin->zperiod;
+            zz[k] = atoms->z[i];
+          }
+  } else {
+    q.assign(atoms->q, atoms->q + 3 * n0);
+    zz.assign(atoms->z, atoms->z + n0);
+  }
+  const int64_t n = (int64_t)zz.size();
+  spec->ctx = ctx;
+  spec->g = make_grid(gin->nx, gin->ny, gin->voltage, gin->xperiod * dx, gin->yperiod * dy,
+                      gin->zperiod * dz, gin->xmin, gin->ymin, gin->zmin, gin->xperiod,
+                      gin->yperiod, gin->zperiod);
+  const Grid& g = spec->g;
+  const int64_t plane = (int64_t)g.nx * g.ny;
+
+  // species in ascending Z (tem.cpp:944-972)
+  std::vector<uint32_t> species(zz.begin(), zz.end());
+  std::sort(species.begin(), species.end());
+  species.erase(std::unique(species.begin(), species.end()), species.end());
+  for (uint32_t z : species)
+    if (!kirkland_params(z)) { set_error("atomic number out of range 1..103"); return MSF_ERR_ARG; }
+
+  MSF_CUDA(cudaSetDevice(ctx->device));
+  MSF_TRY(upload(ctx, &spec->kx, g.kx));
+  MSF_TRY(upload(ctx, &spec->ky, g.ky));
+
+  // per-species LUTs (scatterer_pap.hpp:109-190)
+  DevBuf luts, params;
+  MSF_TRY(ctx->alloc(&luts, sizeof(double) * 2 * plane * std::max<size_t>(1, species.size())));
+  std::vector<double> hp;
+  for (uint32_t z : species) hp.insert(hp.end(), kirkland_params(z), kirkland_params(z) + 12);
+  MSF_TRY(upload(ctx, &params, hp));
+  const double ab_inv = 1 / (g.xpd * g.ypd);
+  const double pref = g.lambda * g.gamma * ab_inv;
+  for (size_t k = 0; k < species.size(); ++k) {
+    MSF_CUDA(launch_lut_synth(luts.as<double>() + 2 * plane * k, spec->kx.as<double>(),
+                              spec->ky.as<double>(), g.nx, g.ny, params.as<double>() + 12 * k,
+                              pref, g.bw_pap * g.bw_pap, g.xmin, g.ymin, ctx->stream));
+  }
+  if (!species.empty())
+    MSF_TRY(fft2d_f64(ctx, g, luts.as<double>(), (int)species.size(), true,
+                      1.0 / std::sqrt((double)(g.nx * (int64_t)g.ny))));
+
+  // slicing (slice.cpp:469-980) and per-atom pixel snaps (slice.cpp:1556-1572)
+  Slicing sl = slice_atoms(n, q.data(), g.zmin, g.zpd, gin->min_slice);
+  spec->n_slices = (int)sl.n();
+  spec->lower = sl.lower;
+  spec->thickness = sl.thickness;
+  spec->counts.resize(sl.n());
+  for (int64_t s = 0; s < sl.n(); ++s) spec->counts[s] = sl.start[s + 1] - sl.start[s];
+  std::vector<int32_t> asx(n), asy(n), asp(n);
+  const double hx = 0.5 * (g.xx[1] - g.xx[0]), hy = 0.5 * (g.yy[1] - g.yy[0]);
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t a = sl.order[k];
+    const int64_t sx = snap(g.xx, q[3 * a], hx, 0), sy = snap(g.yy, q[3 * a + 1], hy, 0);
+    if (sx < 0 || sy < 0) {
+      set_error("atom " + std::to_string(a) + " lies half a pixel or more below the cell "
+                "origin; the reference would index outside its arrays");
+      return MSF_ERR_ARG;
+    }
+    asx[k] = (int32_t)sx;
+    asy[k] = (int32_t)sy;
+    asp[k] = (int32_t)(std::lower_bound(species.begin(), species.end(), zz[a]) - species.begin());
+  }
+  DevBuf dsx, dsy, dsp;
+  MSF_TRY(upload(ctx, &dsx, asx));
+  MSF_TRY(upload(ctx, &dsy, asy));
+  MSF_TRY(upload(ctx, &dsp, asp));
+
+  // band-limit mask (shared by the transmission build and the propagator)
+  std::vector<int32_t> lo, hi;
+  if (!bandlimit_mask(g, g.bw_t, &lo, &hi)) {
+    set_error("band-limit mask is not an interval per column");
+    return MSF_ERR_UNSUPPORTED;
+  }
+  MSF_TRY(upload(ctx, &spec->mask_lo, lo));
+  MSF_TRY(upload(ctx, &spec->mask_hi, hi));
+
+  // transmission functions (slice.cpp:1544-1757)
+  const size_t cbytes = ctx->fp64 ? 16 : 8;
+  MSF_TRY(ctx->alloc(&spec->t, cbytes * plane * std::max<int64_t>(1, sl.n())));
+  DevBuf scratch;
+  if (!ctx->fp64) MSF_TRY(ctx->alloc(&scratch, 16 * plane));
+  PassArgs a;
+  a.batch_stride = plane;
+  a.nb = 1;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  a.mask_lo = spec->mask_lo.as<int32_t>();
+  a.mask_hi = spec->mask_hi.as<int32_t>();
+  for (int64_t s = 0; s < sl.n(); ++s) {
+    double* t64 = ctx->fp64 ? spec->t.as<double>() + 2 * plane * s : scratch.as<double>();
+    const int64_t s0 = sl.start[s], cnt = sl.start[s + 1] - sl.start[s];
+    MSF_CUDA(launch_potential(t64, luts.as<double>(), g.nx, g.ny, dsx.as<int32_t>() + s0,
+                              dsy.as<int32_t>() + s0, dsp.as<int32_t>() + s0, (int)cnt,
+                              ctx->stream));
+    a.psi = t64;
+    MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
+    MSF_CUDA(launch_row(true, ROW_FWD, a, ctx->stream));
+    MSF_TRY(ctx->twiddles(g.nx, true, &a.tw));
+    MSF_CUDA(launch_col(true, COL_FWD_MASK_INV, a, ctx->stream));
+    MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
+    a.scale = 1.0 / g.nxny;
+    MSF_CUDA(launch_row(true, ROW_INV, a, ctx->stream));
+    a.scale = 1.0;
+    if (!ctx->fp64)
+      MSF_CUDA(launch_to_f32(t64, spec->t.as<float>() + 2 * plane * s, 2 * plane, ctx->stream));
+  }
+
+  // propagators (slice.cpp:1293-1363)
+  spec->hprop.clear();
+  for (int64_t s = 0; s < sl.n(); ++s) {
+    std::vector<double> px, py;
+    propagator(g, sl.thickness[s], &px, &py);
+    spec->hprop.insert(spec->hprop.end(), px.begin(), px.end());
+    spec->hprop.insert(spec->hprop.end(), py.begin(), py.end());
+  }
+  if (ctx->fp64) {
+    MSF_TRY(upload(ctx, &spec->prop, spec->hprop));
+  } else {
+    std::vector<float> f(spec->hprop.begin(), spec->hprop.end());
+    MSF_TRY(upload(ctx, &spec->prop, f));
+  }
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  spec->device_bytes = (int64_t)(spec->t.bytes + spec->prop.bytes + spec->mask_lo.bytes +
+                                 spec->mask_hi.bytes + spec->kx.bytes + spec->ky.bytes);
+  spec->seconds_setup = now_s() - t0;
+  return MSF_OK;
+}
+
+msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_optics* o,
+                       DevBuf* probe64) {
+  const Grid& g = spec->g;
+  const int64_t plane = (int64_t)g.nx * g.ny;
+  MSF_TRY(ctx->alloc(probe64, 16 * plane));
+  const double lsq = g.lambda * g.lambda;
+  const double amax_sq = o->alpha_max * o->alpha_max;
+  // probe evaluated at (xx[0], yy[0]) (adfstem.cpp:586-645)
+  MSF_CUDA(launch_probe_synth(probe64->as<double>(), spec->kx.as<double>(),
+                              spec->ky.as<double>(), g.nx, g.ny, o->corrected, o->cs3, o->cs5,
+                              o->defocus, g.lambda, lsq, amax_sq, g.xx[0], g.yy[0],
+                              ctx->stream));
+  // BACKWARD transform, / sqrtNxNy (adfstem.cpp:686-732)
+  MSF_TRY(fft2d_f64(ctx, g, probe64->as<double>(), 1, true, 1.0 / g.s));
+  // Ap = 1/sqrt(sum |psi|^2) (probe_wavefunction.cpp:287-315)
+  DevBuf d_sum;
+  MSF_TRY(ctx->alloc(&d_sum, sizeof(double)));
+  MSF_CUDA(launch_norm2(probe64->as<double>(), plane, d_sum.as<double>(), ctx->stream));
+  double sum = 0;
+  MSF_CUDA(cudaMemcpyAsync(&sum, d_sum.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  const double ap = 1.0 / std::sqrt(sum);
+  MSF_CUDA(launch_scale(probe64->as<double>(), plane, ap, nullptr, ctx->stream));
+  return MSF_OK;
+}
+
+msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int reps,
+                       double* ms_row, double* ms_col) {
+  const Grid& g = spec->g;
+  const int64_t plane = (int64_t)g.nx * g.ny;
+  const bool fp64 = ctx->fp64;
+  const size_t cbytes = fp64 ? 16 : 8;
+  MSF_CUDA(cudaSetDevice(ctx->device));
+  DevBuf psi;
+  MSF_TRY(ctx->alloc(&psi, cbytes * plane * nb));
+  MSF_CUDA(cudaMemsetAsync(psi.p, 0, psi.bytes, ctx->stream));
+  PassArgs row, col;
+  row.psi = col.psi = psi.p;
+  row.batch_stride = col.batch_stride = plane;
+  row.nb = col.nb = nb;
+  row.nx = col.nx = g.nx;
+  row.ny = col.ny = g.ny;
+  MSF_TRY(ctx->twiddles(g.ny, fp64, &row.tw));
+  MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
+  row.inv_s = col.inv_s = 1.0 / g.s;
+  row.trans = spec->t.p;
+  col.mask_lo = spec->mask_lo.as<int32_t>();
+  col.mask_hi = spec->mask_hi.as<int32_t>();
+  col.px = spec->prop.p;
+  col.py = static_cast<const char*>(spec->prop.p) + cbytes * g.nx;
+  std::vector<cudaEvent_t> ev(2 * reps + 2);
+  for (auto& e : ev) MSF_CUDA(cudaEventCreate(&e));
+  // warm-up
+  MSF_CUDA(launch_row(fp64, ROW_SLICE, row, ctx->stream));
+  MSF_CUDA(launch_col(fp64, COL_SLICE, col, ctx->stream));
+  double tr = 0, tc = 0;
+  for (int r = 0; r < reps; ++r) {
+    MSF_CUDA(cudaEventRecord(ev[2 * r], ctx->stream));
+    MSF_CUDA(launch_row(fp64, ROW_SLICE, row, ctx->stream));
+    MSF_CUDA(cudaEventRecord(ev[2 * r + 1], ctx->stream));
+    MSF_CUDA(launch_col(fp64, COL_SLICE, col, ctx->stream));
+    MSF_CUDA(cudaEventRecord(ev[2 * r + 2], ctx->stream));
+  }
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int r = 0; r < reps; ++r) {
+    float a = 0, b = 0;
+    MSF_CUDA(cudaEventElapsedTime(&a, ev[2 * r], ev[2 * r + 1]));
+    MSF_CUDA(cudaEventElapsedTime(&b, ev[2 * r + 1], ev[2 * r + 2]));
+    tr += a;
+    tc += b;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (ms_row) *ms_row = tr / reps;
+  if (ms_col) *ms_col = tc / reps;
+  return MSF_OK;
+}
+
+msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                      const msf_raster* raster, const msf_detect* det, msf_results* res) {
+  if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
+  const Grid& g = spec->g;
+  const int64_t plane = (int64_t)g.nx * g.ny;
+  const bool fp64 = ctx->fp64;
+  const size_t cbytes = fp64 ? 16 : 8;
+  const int S = spec->n_slices;
+  std::vector<double> x_p(raster->x_p, raster->x_p + std::max(0, raster->n_x));
+  std::vector<double> y_p(raster->y_p, raster->y_p + std::max(0, raster->n_y));
+  const int64_t n_probes = (int64_t)x_p.size() * (int64_t)y_p.size();
+  if (n_probes <= 0) { set_error("empty raster"); return MSF_ERR_ARG; }
+  const bool want_adf = det->outputs & MSF_OUT_ADF_IMAGE;
+  const uint32_t fem = det->outputs & MSF_OUT_FEM_MASK;
+  const bool pix_modes = det->outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE |
+                                         MSF_OUT_V_GT17 | MSF_OUT_V_RBAR);
+  MSF_CUDA(cudaSetDevice(ctx->device));
+
+  // probe
+  DevBuf probe64, probe32;
+  MSF_TRY(build_probe(ctx, spec, optics, &probe64));
+  const void* probe = probe64.p;
+  if (!fp64) {
+    MSF_TRY(ctx->alloc(&probe32, 8 * plane));
+    MSF_CUDA(launch_to_f32(probe64.as<double>(), probe32.as<float>(), 2 * plane, ctx->stream));
+    probe = probe32.p;
+  }
+
+  // per-probe pixel shifts
+  std::vector<int32_t> shifts;
+  if (!probe_shifts(g, x_p, y_p, &shifts)) {
+    set_error("a raster position lies half a pixel or more below the cell origin");
+    return MSF_ERR_ARG;
+  }
+  DevBuf d_shifts;
+  MSF_TRY(upload(ctx, &d_shifts, shifts));
+
+  // segments: ring bins (FEM) then the ADF detector annulus
+  Rings rings;
+  if (fem) rings = make_rings(g, det->dr);
+  const int n_k = fem ? rings.n_k : 0;
+  std::vector<int32_t> seg_idx, seg_start{0};
+  if (fem) {
+    seg_idx = rings.pix;
+    for (int k = 0; k < n_k; ++k) seg_start.push_back(rings.start[k + 1]);
+  }
+  const std::vector<int32_t> adf_pix =
+      detector_pixels(g, det->det_inner / g.lambda, det->det_outer / g.lambda);
+  seg_idx.insert(seg_idx.end(), adf_pix.begin(), adf_pix.end());
+  seg_start.push_back((int32_t)seg_idx.size());
+  const int n_seg = n_k + 1;
+  DevBuf d_seg_idx, d_seg_start, d_amp, d_int, d_acc_a, d_acc_i;
+  MSF_TRY(upload(ctx, &d_seg_idx, seg_idx));
+  MSF_TRY(upload(ctx, &d_seg_start, seg_start));
+  MSF_TRY(ctx->alloc(&d_amp, sizeof(double) * n_probes * n_seg));
+  MSF_TRY(ctx->alloc(&d_int, sizeof(double) * n_probes * n_seg));
+  if (pix_modes) {
+    MSF_TRY(ctx->alloc(&d_acc_a, sizeof(double) * plane));
+    MSF_TRY(ctx->alloc(&d_acc_i, sizeof(double) * plane));
+    MSF_CUDA(cudaMemsetAsync(d_acc_a.p, 0, d_acc_a.bytes, ctx->stream));
+    MSF_CUDA(cudaMemsetAsync(d_acc_i.p, 0, d_acc_i.bytes, ctx->stream));
+  }
+
+  // batch of wavefields
+  int B = ctx->batch;
+  if (B <= 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const int64_t cap = (int64_t)(0.5 * (double)free_b) / (int64_t)(cbytes * plane);
+    B = (int)std::max<int64_t>(1, std::min<int64_t>(cap, 64));
+  }
+  B = (int)std::min<int64_t>(B, n_probes);
+  DevBuf psi;
+  MSF_TRY(ctx->alloc(&psi, cbytes * plane * B));
+
+  PassArgs row, col;
+  row.psi = col.psi = psi.p;
+  row.batch_stride = col.batch_stride = plane;
+  row.nx = col.nx = g.nx;
+  row.ny = col.ny = g.ny;
+  MSF_TRY(ctx->twiddles(g.ny, fp64, &row.tw));
+  MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
+  row.inv_s = col.inv_s = 1.0 / g.s;
+  row.probe = probe;
+  row.first_scale = g.nxny / g.s;
+  col.mask_lo = spec->mask_lo.as<int32_t>();
+  col.mask_hi = spec->mask_hi.as<int32_t>();
+  const char* tbase = static_cast<const char*>(spec->t.p);
+  const char* pbase = static_cast<const char*>(spec->prop.p);
+  const size_t prop_stride = cbytes * (g.nx + g.ny);
+
+  // one batch: 2*S fused passes then the reductions
+  auto enqueue_batch = [&](int nb, const int32_t* shifts_dev, double* amp_out,
+                           double* int_out) -> msf_status {
+    row.nb = col.nb = nb;
+    row.shifts = shifts_dev;
+    for (int s = 0; s < S; ++s) {
+      row.trans = tbase + cbytes * plane * s;
+      MSF_CUDA(launch_row(fp64, s == 0 ? ROW_SLICE_FIRST : ROW_SLICE, row, ctx->stream));
+      col.px = pbase + prop_stride * s;
+      col.py = pbase + prop_stride * s + cbytes * g.nx;
+      MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
+    }
+    MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, d_seg_idx.as<int32_t>(),
+                                 d_seg_start.as<int32_t>(), n_seg, amp_out, int_out,
+                                 ctx->stream));
+    if (pix_modes)
+      MSF_CUDA(launch_pixel_accum(fp64, psi.p, plane, nb, plane, d_acc_a.as<double>(),
+                                  d_acc_i.as<double>(), ctx->stream));
+    return MSF_OK;
+  };
+  if (S <= 0) { set_error("specimen has no slices"); return MSF_ERR_ARG; }
+
+  cudaEvent_t ev0, ev1;
+  MSF_CUDA(cudaEventCreate(&ev0));
+  MSF_CUDA(cudaEventCreate(&ev1));
+  MSF_CUDA(cudaEventRecord(ev0, ctx->stream));
+  cudaGraphExec_t graph_exec = nullptr;
+  DevBuf stage_shift, stage_amp, stage_int;
+  const bool use_graph = ctx->graphs && n_probes / B >= 2;
+  if (use_graph) {
+    MSF_TRY(ctx->alloc(&stage_shift, sizeof(int32_t) * 2 * B));
+    MSF_TRY(ctx->alloc(&stage_amp, sizeof(double) * B * n_seg));
+    MSF_TRY(ctx->alloc(&stage_int, sizeof(double) * B * n_seg));
+  }
+  msf_status st = MSF_OK;
+  for (int64_t p0 = 0; p0 < n_probes && st == MSF_OK; p0 += B) {
+    const int nb = (int)std::min<int64_t>(B, n_probes - p0);
+    if (use_graph && nb == B && p0 > 0) {
+      MSF_CUDA(cudaMemcpyAsync(stage_shift.p, d_shifts.as<int32_t>() + 2 * p0,
+                               sizeof(int32_t) * 2 * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (!graph_exec) {
+        cudaGraph_t graph;
+        MSF_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_batch(nb, stage_shift.as<int32_t>(), stage_amp.as<double>(),
+                           stage_int.as<double>());
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (st != MSF_OK) break;
+        MSF_CUDA(ce);
+        MSF_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+        cudaGraphDestroy(graph);
+      }
+      MSF_CUDA(cudaGraphLaunch(graph_exec, ctx->stream));
+      MSF_CUDA(cudaMemcpyAsync(d_amp.as<double>() + p0 * n_seg, stage_amp.p,
+                               sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+      MSF_CUDA(cudaMemcpyAsync(d_int.as<double>() + p0 * n_seg, stage_int.p,
+                               sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    } else {
+      st = enqueue_batch(nb, d_shifts.as<int32_t>() + 2 * p0, d_amp.as<double>() + p0 * n_seg,
+                         d_int.as<double>() + p0 * n_seg);
+    }
+  }
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (st != MSF_OK) return st;
+  MSF_CUDA(cudaEventRecord(ev1, ctx->stream));
+
+  // copy back
+  std::vector<double> amp((size_t)n_probes * n_seg), inten((size_t)n_probes * n_seg);
+  MSF_CUDA(cudaMemcpyAsync(amp.data(), d_amp.p, amp.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  MSF_CUDA(cudaMemcpyAsync(inten.data(), d_int.p, inten.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<double> acc_a, acc_i;
+  if (pix_modes) {
+    acc_a.resize(plane);
+    acc_i.resize(plane);
+    MSF_CUDA(cudaMemcpyAsync(acc_a.data(), d_acc_a.p, plane * sizeof(double),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    MSF_CUDA(cudaMemcpyAsync(acc_i.data(), d_acc_i.p, plane * sizeof(double),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  std::vector<float> last32;
+  if (res->final_psi) {
+    const int last = (int)((n_probes - 1) % B);
+    if (fp64) {
+      MSF_CUDA(cudaMemcpyAsync(res->final_psi, psi.as<double>() + 2 * plane * last,
+                               16 * plane, cudaMemcpyDeviceToHost, ctx->stream));
+    } else {
+      last32.resize(2 * plane);
+      MSF_CUDA(cudaMemcpyAsync(last32.data(), psi.as<float>() + 2 * plane * last, 8 * plane,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0;
+  MSF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (!last32.empty())
+    for (int64_t k = 0; k < 2 * plane; ++k) res->final_psi[k] = last32[k];
+  res->seconds_raster = 1e-3 * ms;
+  res->seconds_setup = 0;
+  res->probe_slices = n_probes * S;
+  {
+    const int64_t n_batches = (n_probes + B - 1) / B;
+    // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:
+    // 2*S slice passes, the segment sums and (pixel modes) the accumulation
+    res->kernel_launches = 5 + (fp64 ? 0 : 1) + n_batches * (2 * S + 1 + (pix_modes ? 1 : 0));
+    ctx->d2h_bytes += (int64_t)(8 + 2 * amp.size() * sizeof(double)) +
+                      (pix_modes ? 16 * plane : 0) +
+                      (res->final_psi ? (int64_t)cbytes * plane : 0);
+  }
+
+  if (want_adf && res->adf_image)
+    for (int64_t p = 0; p < n_probes; ++p) res->adf_image[p] = inten[p * n_seg + n_k];
+
+  // ---- FEM statistics on the host, in the reference's order -----------
+  res->n_k = n_k;
+  if (!fem) return MSF_OK;
+  if (n_k > res->cap_k) {
+    set_error("results.cap_k is smaller than the number of k bins (" + std::to_string(n_k) + ")");
+    return MSF_ERR_ARG;
+  }
+  std::vector<uint8_t> inside(n_k);
+  for (int k = 0; k < n_k; ++k)
+    inside[k] = (g.lambda * rings.bounds[k + 1] <= optics->alpha_max);  // adfstem.cpp:2518
+  const std::vector<int32_t>& cnt = rings.counts;
+  for (int k = 0; k < n_k; ++k) {
+    if (res->k_lower) res->k_lower[k] = rings.bounds[k];
+    if (res->bin_counts) res->bin_counts[k] = cnt[k];
+  }
+  const double n_r = (double)(size_t)n_probes;
+  if (det->outputs & (MSF_OUT_V_OMEGA | MSF_OUT_VBAR_R)) {
+    std::vector<double> sa2(n_k, 0.0), sa(n_k, 0.0), vs(n_k, 0.0);
+    for (int64_t p = 0; p < n_probes; ++p) {
+      const double* ring = &amp[p * n_seg];
+      const double* ring2 = &inten[p * n_seg];
+      for (int k = 0; k < n_k; ++k) {
+        const double S1 = inside[k] ? 0.0 : ring[k];
+        const double S2 = inside[k] ? 0.0 : ring2[k];
+        sa2[k] += (S1 * S1) / (cnt[k] * cnt[k]);   // adfstem.cpp:2585-2601
+        sa[k] += S1 / cnt[k];
+        vs[k] += ((S2 / cnt[k]) / ((S1 * S1) / (cnt[k] * cnt[k]))) - 1.0;  // :2735-2748
+      }
+    }
+    for (int k = 0; k < n_k; ++k) {
+      if (res->v_omega && (det->outputs & MSF_OUT_V_OMEGA))
+        res->v_omega[k] = (sa[k] == 0.0) ? 0.0 : (n_r * sa2[k] / (sa[k] * sa[k])) - 1.0;
+      if (res->vbar_r && (det->outputs & MSF_OUT_VBAR_R)) res->vbar_r[k] = vs[k] / n_r;
+    }
+  }
+  if (pix_modes) {  // adfstem.cpp:2926-3612
+    std::vector<double> mean_a(plane), mean_sq(plane), mean_i(plane), var(plane);
+    for (int64_t p = 0; p < plane; ++p) {
+      mean_a[p] = acc_a[p] / n_r;
+      mean_sq[p] = mean_a[p] * mean_a[p];
+      mean_i[p] = acc_i[p] / n_r;
+    }
+    if (res->mean_amplitude) std::memcpy(res->mean_amplitude, mean_a.data(), plane * 8);
+    if (res->mean_intensity) std::memcpy(res->mean_intensity, mean_i.data(), plane * 8);
+    auto ring_sum = [&](const std::vector<double>& v, std::vector<double>* out) {
+      out->assign(n_k, 0.0);
+      for (int k = 0; k < n_k; ++k) {
+        double s = 0.0;
+        for (int32_t q = rings.start[k]; q < rings.start[k + 1]; ++q) s += v[rings.pix[q]];
+        (*out)[k] = inside[k] ? 0.0 : s;
+      }
+    };
+    std::vector<double> r1, r2, r3;
+    ring_sum(mean_i, &r1);
+    ring_sum(mean_sq, &r2);
+    ring_sum(mean_a, &r3);
+    for (int k = 0; k < n_k; ++k) {
+      const double c = (double)cnt[k];
+      const double cc = (double)(cnt[k] * cnt[k]);
+      if (res->v_gt17 && (det->outputs & MSF_OUT_V_GT17)) res->v_gt17[k] = (r1[k] / c) / (r2[k] / c);
+      if (res->v_re && (det->outputs & MSF_OUT_V_RE))
+        res->v_re[k] = ((r1[k] / c) / (r3[k] * r3[k] / cc)) - 1.0;
+      if (res->v_rbar && (det->outputs & MSF_OUT_V_RBAR))
+        res->v_rbar[k] = ((r2[k] / c) / (r3[k] * r3[k] / cc)) - 1.0;
+    }
+    if (res->omega_vimage && (det->outputs & MSF_OUT_OMEGA_VIMAGE)) {
+      const double lsq = g.lambda * g.lambda, amax_sq = optics->alpha_max * optics->alpha_max;
+      for (int i = 0; i < g.nx; ++i)
+        for (int j = 0; j < g.ny; ++j) {
+          const int64_t p = j + (int64_t)g.ny * i;
+          var[p] = (mean_i[p] / (mean_a[p] * mean_a[p])) - 1.0;
+          const double ksqr = std::pow(g.kx[i], 2) + std::pow(g.ky[j], 2);
+          if (lsq * ksqr <= amax_sq) var[p] = 0.0;
+        }
+      std::vector<double> r4;
+      ring_sum(var, &r4);
+      for (int k = 0; k < n_k; ++k) res->omega_vimage[k] = r4[k] / cnt[k];
+    }
+  }
+  return MSF_OK;
+}
+
+}  // namespace msf

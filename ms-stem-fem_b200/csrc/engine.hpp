@@ -1,0 +1,78 @@
+// Device-side engine behind the C ABI: contexts, specimens, raster runs.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "msf.h"
+#include "setup.hpp"
+
+namespace msf {
+
+void set_error(const std::string& msg);
+
+// Owning device allocation that counts against its context's budget.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int64_t* counter = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    release();
+    p = o.p; bytes = o.bytes; counter = o.counter;
+    o.p = nullptr; o.bytes = 0; o.counter = nullptr;
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release();
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace msf
+
+struct msf_context {
+  int device = 0;
+  bool fp64 = true;
+  int batch = 0;
+  bool graphs = true;
+  int64_t budget = 0;
+  int64_t allocated = 0;
+  int64_t h2d_bytes = 0, d2h_bytes = 0;
+  cudaStream_t stream = nullptr;
+  std::map<int, msf::DevBuf> tw64, tw32;  // twiddle tables per length
+  msf_status alloc(msf::DevBuf* b, size_t bytes);
+  msf_status twiddles(int n, bool fp64, const void** out);
+};
+
+struct msf_specimen {
+  msf_context* ctx = nullptr;
+  msf::Grid g;
+  std::vector<double> lower, thickness;
+  std::vector<int64_t> counts;
+  int n_slices = 0;
+  msf::DevBuf t;              // [slice][nx][ny] complex, context precision
+  msf::DevBuf prop;           // [slice] {px[nx], py[ny]} complex, context precision
+  msf::DevBuf mask_lo, mask_hi;
+  msf::DevBuf kx, ky;         // FP64 domains for device set-up kernels
+  std::vector<double> hprop;  // FP64 propagators, host copy
+  double seconds_setup = 0;
+  int64_t device_bytes = 0;
+};
+
+namespace msf {
+msf_status build_specimen(msf_context* ctx, const msf_grid* grid, const msf_atoms* atoms,
+                          msf_specimen* spec);
+msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                      const msf_raster* raster, const msf_detect* detect, msf_results* res);
+msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                       DevBuf* probe64);
+msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int reps,
+                       double* ms_row, double* ms_col);
+}  // namespace msf

@@ -1,0 +1,205 @@
+// Register-resident Stockham FFT building blocks for sm_100a.
+//
+// A "line" is one 1-D transform of length N (a row along y, or a column
+// along x, of the [x][y] wavefield).  It is held by T = N/E threads, each
+// owning E elements in registers: thread t holds element t + T*m in slot m,
+// on entry and on exit, for every shape below.  Between radix stages the
+// line is exchanged through a padded shared-memory buffer; inside a stage
+// each thread runs E/R radix-R butterflies fully in registers, with
+// compile-time constant twiddles inside the butterfly and table twiddles
+// (from an FP64-computed table) between stages.
+//
+// Because entry and exit layouts coincide, an inverse transform, a
+// point-wise product and a forward transform chain with no data movement
+// between them; this is what lets one kernel pass fuse "inverse FFT along y,
+// multiply by the transmission function, forward FFT along y".
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <type_traits>
+
+namespace msf {
+
+#include "unit_roots.inc"
+
+template <typename R> struct CxT;
+template <> struct CxT<float> { using type = float2; };
+template <> struct CxT<double> { using type = double2; };
+template <typename R> using Cx = typename CxT<R>::type;
+
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return C{a.x + b.x, a.y + b.y}; }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return C{a.x - b.x, a.y - b.y}; }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+// a * conj(b)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
+  return C{a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) {
+  return C{a.x * s, a.y * s};
+}
+
+template <int I> using ic = std::integral_constant<int, I>;
+
+// Compile-time loop: f(ic<B>), f(ic<B+S>), ... while < E.
+template <int B, int E, int S = 1, typename F>
+__device__ __forceinline__ void sfor(F&& f) {
+  if constexpr (B < E) {
+    f(ic<B>{});
+    sfor<B + S, E, S>(f);
+  }
+}
+
+// a * W_M^K, W_M = e^{-2 pi i / M} (forward) or its conjugate (inverse).
+template <int K, int M, bool INV, typename C>
+__device__ __forceinline__ C twc(C a) {
+  static_assert(M <= 64 && 64 % M == 0, "butterfly radix must divide 64");
+  using R = decltype(a.x);
+  constexpr int k = (K * (64 / M)) & 63;
+  if constexpr (k == 0) {
+    return a;
+  } else if constexpr (k == 16) {  // forward -i, inverse +i
+    return INV ? C{-a.y, a.x} : C{a.y, -a.x};
+  } else if constexpr (k == 32) {
+    return C{-a.x, -a.y};
+  } else if constexpr (k == 48) {  // forward +i, inverse -i
+    return INV ? C{a.y, -a.x} : C{-a.y, a.x};
+  } else {
+    constexpr R c = (R)cos64(k);
+    constexpr R s = (R)sin64(k);
+    if constexpr (INV) return C{a.x * c - a.y * s, a.x * s + a.y * c};
+    else return C{a.x * c + a.y * s, a.y * c - a.x * s};
+  }
+}
+
+__host__ __device__ constexpr int bitrev(int x, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((x >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+__host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
+
+// One radix-2 decimation-in-frequency layer over u[0..R) with span SPAN,
+// then the remaining layers.
+template <int R, int SPAN, bool INV, typename C>
+__device__ __forceinline__ void dif_layers(C (&u)[R]) {
+  sfor<0, R, 2 * SPAN>([&](auto base) {
+    sfor<0, SPAN>([&](auto k) {
+      constexpr int a = decltype(base)::value + decltype(k)::value;
+      C x = u[a], y = u[a + SPAN];
+      u[a] = cadd(x, y);
+      u[a + SPAN] = twc<decltype(k)::value, 2 * SPAN, INV>(csub(x, y));
+    });
+  });
+  if constexpr (SPAN > 1) dif_layers<R, SPAN / 2, INV>(u);
+}
+
+// In-place length-R DFT of v[OFF + r*STR], r < R, natural order in and out.
+template <int R, bool INV, int OFF, int STR, typename C, int E>
+__device__ __forceinline__ void dft(C (&v)[E]) {
+  if constexpr (R > 1) {
+    C u[R];
+    sfor<0, R>([&](auto r) { u[decltype(r)::value] = v[OFF + decltype(r)::value * STR]; });
+    dif_layers<R, R / 2, INV>(u);
+    constexpr int bits = ilog2(R);
+    sfor<0, R>([&](auto p) {
+      constexpr int q = decltype(p)::value;
+      v[OFF + bitrev(q, bits) * STR] = u[q];
+    });
+  }
+}
+
+// ---------------------------------------------------------------- shapes --
+// FFT length N: E elements per thread, S radix stages R0..R{S-1} (each R
+// divides E).  FP64 keeps E <= 16 to bound register use.
+template <int N, typename Real> struct Shape;
+#define MSF_SHAPE(N_, REAL_, E_, S_, R0_, R1_, R2_)                          \
+  template <> struct Shape<N_, REAL_> {                                       \
+    static constexpr int N = N_, E = E_, S = S_, T = N_ / E_;                 \
+    static constexpr int R0 = R0_, R1 = R1_, R2 = R2_;                        \
+    __host__ __device__ static constexpr int radix(int s) { return s == 0 ? R0 : s == 1 ? R1 : R2; } \
+    __host__ __device__ static constexpr int ns(int s) {                                          \
+      return s == 0 ? 1 : s == 1 ? R0 : R0 * R1;                              \
+    }                                                                         \
+  };
+MSF_SHAPE(64, float, 8, 2, 8, 8, 1)
+MSF_SHAPE(128, float, 16, 2, 16, 8, 1)
+MSF_SHAPE(256, float, 16, 2, 16, 16, 1)
+MSF_SHAPE(512, float, 32, 2, 32, 16, 1)
+MSF_SHAPE(1024, float, 32, 2, 32, 32, 1)
+MSF_SHAPE(2048, float, 32, 3, 32, 8, 8)
+MSF_SHAPE(4096, float, 16, 3, 16, 16, 16)
+MSF_SHAPE(64, double, 8, 2, 8, 8, 1)
+MSF_SHAPE(128, double, 16, 2, 16, 8, 1)
+MSF_SHAPE(256, double, 16, 2, 16, 16, 1)
+MSF_SHAPE(512, double, 8, 3, 8, 8, 8)
+MSF_SHAPE(1024, double, 16, 3, 16, 16, 4)
+MSF_SHAPE(2048, double, 16, 3, 16, 16, 8)
+MSF_SHAPE(4096, double, 16, 3, 16, 16, 16)
+#undef MSF_SHAPE
+
+// Shared-memory line layout: one padding slot every R0 elements keeps the
+// stride-R0 writes of the first exchange conflict-free; the odd line stride
+// keeps neighbouring lines (columns) on different banks.
+template <class Sh> struct Smem {
+  static constexpr int pad_shift = ilog2(Sh::R0);
+  static constexpr int stride = Sh::N + (Sh::N >> pad_shift) + 1;
+  __device__ __forceinline__ static int at(int a) { return a + (a >> pad_shift); }
+};
+
+// Transform one line in place.  v[m] holds element t + T*m on entry and
+// X[t + T*m] on exit.  `sm` is this line's shared buffer (Smem<Sh>::stride
+// elements), `tw` the table e^{-2 pi i m / N}, m < N, and `sync` a barrier
+// over all threads that share `sm` lines with this one.
+template <class Sh, bool INV, typename C, class Sync>
+__device__ __forceinline__ void fft_line(C (&v)[Sh::E], C* __restrict__ sm,
+                                         int t, const C* __restrict__ tw,
+                                         Sync&& sync) {
+  constexpr int N = Sh::N, E = Sh::E, T = Sh::T;
+  using SM = Smem<Sh>;
+  sfor<0, Sh::S>([&](auto sI) {
+    constexpr int s = decltype(sI)::value;
+    constexpr int R = Sh::radix(s);
+    constexpr int NB = E / R;
+    constexpr int NS = Sh::ns(s);
+    if constexpr (s > 0) {
+      sfor<0, NB>([&](auto bI) {
+        constexpr int b = decltype(bI)::value;
+        const int j = t + T * b;
+        sfor<0, R>([&](auto rI) {
+          constexpr int r = decltype(rI)::value;
+          v[b + r * NB] = sm[SM::at(j + r * (N / R))];
+        });
+      });
+    }
+    sfor<0, NB>([&](auto bI) {
+      constexpr int b = decltype(bI)::value;
+      if constexpr (NS > 1) {
+        const int j = t + T * b;
+        const int k = j & (NS - 1);
+        sfor<1, R>([&](auto rI) {
+          constexpr int r = decltype(rI)::value;
+          const C w = __ldg(&tw[r * k * (N / (NS * R))]);
+          v[b + r * NB] = INV ? cmulc(v[b + r * NB], w) : cmul(v[b + r * NB], w);
+        });
+      }
+      dft<R, INV, b, NB>(v);
+    });
+    if constexpr (s + 1 < Sh::S) {
+      sync();
+      sfor<0, NB>([&](auto bI) {
+        constexpr int b = decltype(bI)::value;
+        const int j = t + T * b;
+        const int base = (j / NS) * NS * R + (j & (NS - 1));
+        sfor<0, R>([&](auto rI) {
+          constexpr int r = decltype(rI)::value;
+          sm[SM::at(base + r * NS)] = v[b + r * NB];
+        });
+      });
+      sync();
+    }
+  });
+}
+
+}  // namespace msf

@@ -1,0 +1,753 @@
+// Drop-in front end: the reference's command line, parameter file, specimen
+// readers and output writers, on top of the C ABI.
+//
+//   parse_args         read_cmdline_options   (tem_io.cpp:5277-5720)
+//   parse_param_file   read_parameter_file    (tem_io.cpp:4063-4626)
+//   check_flags        check_runtime_flags    (tem_io.cpp:5858-6169)
+//   read_lammps        read_position_lammps_data_file (tem_io.cpp:36-1028)
+//   finish_job         tem.cpp:405-1378 (lambda, cut-offs, defaults, raster,
+//                      Scherzer conditions, output prefix)
+//   write_outputs      output_variance_to_txt (io_txt.cpp:30-94) and
+//                      output_stem_image (write_tif.cpp:1552-1605,
+//                      write_tif.hpp:143-335)
+// Quirks of the reference's parser are kept where they change what a
+// command line means (--detectorangles reads its first number twice,
+// --mtf_file does not consume its argument, the parameter file resets the
+// -m flag); they are marked where they occur.
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "msf.h"
+#include "setup.hpp"
+
+namespace msf {
+const char* last_error();
+}
+
+struct Flags {
+  unsigned m = 0, pf = 0, o = 0, a = 0, defocus = 0, spread = 0, adfstem_corrected = 0,
+           adfstem_uncorrected = 0, bfctem_corrected = 0, bfctem_uncorrected = 0, fem = 0,
+           gt17 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, rva = 0, scherzer_defocus = 0,
+           scherzer_alphamax = 0, scherzer_cs3 = 0, cs3 = 0, cs5 = 0, alpha_max = 0,
+           adfstem_detector_angles = 0, raster_spacing = 0, mtf_file = 0, mtf_resolution = 0,
+           pap_tif = 0, dupe = 0, image_output = 0, diffraction_output = 0, netcdf_images = 0,
+           netcdf_variance = 0, nx = 0, ny = 0, microscope_voltage = 0, debug = 0,
+           correlograph = 0, correlograph_variance = 0, correlograph_everyimage = 0,
+           correlograph_everytxt = 0, lammps_preTEM_file = 0, lammps_TEM_steps = 0,
+           lammps_TEM_samples = 0, fail = 0;
+};
+
+struct msf_job {
+  Flags flags;
+  std::string program = "ms-stem-fem";
+  std::string model_file, output_prefix, full_prefix;
+  int nx = 0, ny = 0;
+  double VV = 0, defocus = 0, alpha_max = 0, defocus_spread = 1.0, cond_angle = 0, Cs3 = 0,
+         Cs5 = 0, det_inner = 0, det_outer = 0, raster_spacing = 0, mtf_resolution = 0;
+  double dr = 0.70710678118654746;  // tem.cpp:186
+  double min_slice = 1.0;           // tem.cpp:188
+  unsigned dupe_x = 1, dupe_y = 1, dupe_z = 1;
+  std::string lammps_pre;
+  unsigned lammps_steps = 0, lammps_samples = 0;
+  // specimen
+  std::vector<double> q;
+  std::vector<uint32_t> z;
+  double xperiod = 0, yperiod = 0, zperiod = 0, xmin = 0, ymin = 0, zmin = 0;
+  // derived
+  double lambda = 0, gamma = 0;
+  std::vector<double> x_p, y_p;
+  bool corrected = false;
+  double cs3_used = 0;
+  std::string messages;  // what the reference would print on failure
+};
+
+namespace {
+
+std::string lower(std::string s) {
+  std::transform(s.begin(), s.end(), s.begin(), [](unsigned char c) { return std::tolower(c); });
+  return s;
+}
+
+template <typename T>
+void parse_into(const std::string& s, T& v) {
+  std::istringstream is(s);
+  is >> v;  // failed extraction leaves 0 (C++11), as the reference's istringstream
+}
+
+bool blank(const std::string& l) { return l.find_first_not_of(" \t") == std::string::npos; }
+
+// getline that skips whitespace-only lines, as the reference's readers do
+bool next_line(std::istream& in, std::string& line) {
+  if (!(std::getline(in, line) && in.good())) return false;
+  while (blank(line)) {
+    if (!std::getline(in, line)) return false;
+  }
+  return true;
+}
+
+bool parse_param_file(const std::string& path, msf_job* j) {
+  Flags& f = j->flags;
+  std::ifstream in(path.c_str());
+  if (!in.is_open()) return false;
+  std::string line;
+  while (std::getline(in, line) && in.good()) {
+    while (blank(line)) {
+      if (!std::getline(in, line)) break;
+    }
+    if (blank(line)) break;
+    std::istringstream ls(line);
+    std::string key;
+    ls >> key;
+    key = lower(key);
+    if (key == "debug") f.debug = 1;
+    else if (key == "output_prefix") { ls >> j->output_prefix; f.o = 1; }
+    else if (key == "samples_x") { int v = 0; ls >> v; j->nx = v; f.nx = 1; }
+    else if (key == "samples_y") { int v = 0; ls >> v; j->ny = v; f.ny = 1; }
+    else if (key == "model_file") { ls >> j->model_file; f.a = 1; }
+    else if (key == "microscope_voltage") { ls >> j->VV; f.microscope_voltage = 1; }
+    else if (key == "scherzer_defocus") f.scherzer_defocus = 1;
+    else if (key == "scherzer_alphamax") f.scherzer_alphamax = 1;
+    else if (key == "scherzer_cs3") f.scherzer_cs3 = 1;
+    else if (key == "defocus") { ls >> j->defocus; f.defocus = 1; }
+    else if (key == "alphamax") { ls >> j->alpha_max; f.alpha_max = 1; }
+    else if (key == "spread") { ls >> j->defocus_spread >> j->cond_angle; f.spread = 1; }
+    else if (key == "cs3") { ls >> j->Cs3; f.cs3 = 1; }
+    else if (key == "cs5") { ls >> j->Cs5; f.cs5 = 1; }
+    else if (key == "detectorangles") {
+      ls >> j->det_inner >> j->det_outer;
+      if (j->det_inner > j->det_outer) std::swap(j->det_inner, j->det_outer);
+      f.adfstem_detector_angles = 1;
+    } else if (key == "mtf_file") {
+      j->messages += "Error, the MTF detector model (mtf_file) is not supported by this build\n";
+      f.fail = 1;
+    } else if (key == "mtf_sampling_rate") {
+      j->mtf_resolution = 0;
+      if (!ls.eof()) ls >> j->mtf_resolution;
+      f.mtf_resolution = j->mtf_resolution == 0 ? 0 : 1;
+    } else if (key == "raster_spacing") { ls >> j->raster_spacing; f.raster_spacing = 1; }
+    else if (key == "adfstemuncorrfem") { f.adfstem_uncorrected = 1; f.fem = 1; }
+    else if (key == "adfstemcorrfem") { f.adfstem_corrected = 1; f.fem = 1; }
+    else if (key == "v_gt17") f.gt17 = 1;
+    else if (key == "v_omega") f.d1 = 1;
+    else if (key == "vbar_r") f.d2 = 1;
+    else if (key == "v_re") f.d3 = 1;
+    else if (key == "omega_vimage") f.d4 = 1;
+    else if (key == "v_rbar") f.rva = 1;
+    else if (key == "adfstemcorr") f.adfstem_corrected = 1;
+    else if (key == "adfstemuncorr") f.adfstem_uncorrected = 1;
+    else if (key == "bfctemcorr") f.bfctem_corrected = 1;
+    else if (key == "bfctemuncorr") f.bfctem_uncorrected = 1;
+    else if (key == "paptif") f.pap_tif = 1;
+    else if (key == "dupe") f.dupe = 1;
+    else if (key == "dr") ls >> j->dr;
+    else if (key == "minslice") ls >> j->min_slice;
+    else if (key == "images") f.image_output = 1;
+    else if (key == "diffractionimages") f.diffraction_output = 1;
+    else if (key == "netcdfimages") f.netcdf_images = 1;
+    else if (key == "netcdfvariance") f.netcdf_variance = 1;
+    else if (key == "correlograph") f.correlograph = 1;
+    else if (key == "correlograph_variance") { f.correlograph_variance = 1; f.correlograph = 1; }
+    else if (key == "correlograph_everyimage") { f.correlograph_everyimage = 1; f.correlograph = 1; }
+    else if (key == "correlograph_everytxt") { f.correlograph_everytxt = 1; f.correlograph = 1; }
+    else if (key == "lammps_pretem_file_name") { ls >> j->lammps_pre; f.lammps_preTEM_file = 1; }
+    else if (key == "lammps_tem_steps") { ls >> j->lammps_steps; f.lammps_TEM_steps = 1; }
+    else if (key == "lammps_tem_samples") { ls >> j->lammps_samples; f.lammps_TEM_samples = 1; }
+    else {
+      j->messages += "Error, unexpected keyword in parameter file : " + key + "\n";
+      return false;
+    }
+  }
+  if (f.fem && !(f.d1 || f.d2 || f.d3 || f.d4 || f.gt17 || f.rva || f.correlograph)) f.d1 = 1;
+  return f.fail == 0;
+}
+
+void parse_args(const std::vector<std::string>& args, msf_job* j) {
+  Flags& f = j->flags;
+  for (size_t idx = 1; idx < args.size(); ++idx) {
+    const std::string& a = args[idx];
+    auto has = [&](size_t k) { return idx + k < args.size(); };
+    if (a == "--parameter_file") {
+      std::string name;
+      if (has(1)) name = args[idx + 1];
+      if (!parse_param_file(name, j)) {
+        j->messages += "Error, could not read parameter file : " + name + "\n";
+        f.fail = 1;
+      }
+      // quirk kept: -m given earlier is re-derived from the file's keys
+      f.m = (f.microscope_voltage && f.nx && f.ny) ? 1 : 0;
+      f.pf = 1;
+      idx += 1;
+    } else if (a == "--mtf_file") {
+      // the reference reads the file but does not consume the argument
+      j->messages += "Error, the MTF detector model (--mtf_file) is not supported by this build\n";
+      f.fail = 1;
+    } else if (a == "--mtf_sampling_rate") {
+      j->mtf_resolution = 0;
+      if (has(1)) { parse_into(args[idx + 1], j->mtf_resolution); idx += 1; }
+      f.mtf_resolution = j->mtf_resolution <= 0 ? 0 : 1;
+    } else if (a == "--debug") f.debug = 1;
+    else if (a == "--output_prefix") {
+      if (has(1)) { j->output_prefix = args[idx + 1]; f.o = 1; }
+      idx += 1;
+    } else if (a == "-m") {
+      int nx = 0, ny = 0;
+      if (has(1)) parse_into(args[idx + 1], nx);
+      if (has(2)) parse_into(args[idx + 2], ny);
+      if (has(3)) parse_into(args[idx + 3], j->VV);
+      j->nx = nx;
+      j->ny = ny;
+      f.m = 1;
+      idx += 3;
+    } else if (a == "-a") {
+      if (has(1)) j->model_file = args[idx + 1];
+      f.a = 1;
+      idx += 1;
+    } else if (a == "--scherzer_defocus") f.scherzer_defocus = 1;
+    else if (a == "--scherzer_alphamax") f.scherzer_alphamax = 1;
+    else if (a == "--scherzer_cs3") f.scherzer_cs3 = 1;
+    else if (a == "--defocus") { if (has(1)) parse_into(args[idx + 1], j->defocus); f.defocus = 1; idx += 1; }
+    else if (a == "--alphamax") { if (has(1)) parse_into(args[idx + 1], j->alpha_max); f.alpha_max = 1; idx += 1; }
+    else if (a == "--spread") {
+      if (has(1)) parse_into(args[idx + 1], j->defocus_spread);
+      if (has(2)) parse_into(args[idx + 2], j->cond_angle);
+      f.spread = 1;
+      idx += 2;
+    } else if (a == "--cs3") { if (has(1)) parse_into(args[idx + 1], j->Cs3); f.cs3 = 1; idx += 1; }
+    else if (a == "--cs5") { if (has(1)) parse_into(args[idx + 1], j->Cs5); f.cs5 = 1; idx += 1; }
+    else if (a == "--detectorangles") {
+      // quirk kept (tem_io.cpp:5529-5545): both angles read from args[idx+1]
+      // and only one argument consumed
+      if (has(1)) parse_into(args[idx + 1], j->det_inner);
+      if (has(2)) parse_into(args[idx + 1], j->det_outer);
+      if (j->det_inner > j->det_outer) std::swap(j->det_inner, j->det_outer);
+      f.adfstem_detector_angles = 1;
+      idx += 1;
+    } else if (a == "--rasterspacing") {
+      if (has(1)) parse_into(args[idx + 1], j->raster_spacing);
+      f.raster_spacing = 1;
+      idx += 1;
+    } else if (a == "--adfstemuncorrfem") { f.adfstem_uncorrected = 1; f.fem = 1; }
+    else if (a == "--adfstemcorrfem") { f.adfstem_corrected = 1; f.fem = 1; }
+    else if (a == "--V_gt17") f.gt17 = 1;
+    else if (a == "--V_omega") f.d1 = 1;
+    else if (a == "--Vbar_r") f.d2 = 1;
+    else if (a == "--V_re") f.d3 = 1;
+    else if (a == "--Omega_vimage") f.d4 = 1;
+    else if (a == "--V_rbar") f.rva = 1;
+    else if (a == "--adfstemcorr") f.adfstem_corrected = 1;
+    else if (a == "--adfstemuncorr") f.adfstem_uncorrected = 1;
+    else if (a == "--bfctemcorr") f.bfctem_corrected = 1;
+    else if (a == "--bfctemuncorr") f.bfctem_uncorrected = 1;
+    else if (a == "--paptif") f.pap_tif = 1;
+    else if (a == "--dupe") {
+      if (has(3)) parse_into(args[idx + 1], j->dupe_x);
+      if (idx + 2 < args.size()) parse_into(args[idx + 2], j->dupe_y);
+      if (idx + 3 < args.size()) parse_into(args[idx + 3], j->dupe_z);
+      f.dupe = 1;
+      idx += 3;
+    } else if (a == "--dr") { if (has(1)) parse_into(args[idx + 1], j->dr); idx += 1; }
+    else if (a == "--minslice") { if (has(1)) parse_into(args[idx + 1], j->min_slice); idx += 1; }
+    else if (a == "--images") f.image_output = 1;
+    else if (a == "--netcdfimages") f.netcdf_images = 1;
+    else if (a == "--netcdfvariance") f.netcdf_variance = 1;
+    else if (a == "--correlograph") f.correlograph = 1;
+    else if (a == "--correlograph_variance") { f.correlograph_variance = 1; f.correlograph = 1; }
+    else if (a == "--correlograph_everyimage") { f.correlograph_everyimage = 1; f.correlograph = 1; }
+    else if (a == "--correlograph_everytxt") { f.correlograph_everytxt = 1; f.correlograph = 1; }
+    else if (a == "--lammps_preTEM_file_name") {
+      if (has(1)) { j->lammps_pre = args[idx + 1]; f.lammps_preTEM_file = 1; }
+      idx += 1;
+    } else if (a == "--lammps_TEM_steps") {
+      if (has(1)) { parse_into(args[idx + 1], j->lammps_steps); f.lammps_TEM_steps = 1; }
+      idx += 1;
+    } else if (a == "--lammps_TEM_samples") {
+      if (has(1)) { parse_into(args[idx + 1], j->lammps_samples); f.lammps_TEM_samples = 1; }
+      idx += 1;
+    } else {
+      j->messages += "Error, unexpected argument : " + a + "\n";
+      f.fail = 1;
+    }
+  }
+  if (!f.gt17 && !f.d1 && !f.d2 && !f.d3 && !f.d4 && !f.rva && !f.correlograph) f.d1 = 1;
+}
+
+// check_runtime_flags (tem_io.cpp:5858-6169)
+void check_flags(msf_job* j) {
+  Flags& f = j->flags;
+  const bool ok =
+      f.o && f.m && !((f.adfstem_corrected || f.bfctem_corrected) && !(f.cs5 && (f.scherzer_cs3 || f.cs3))) &&
+      !((f.adfstem_uncorrected || f.bfctem_uncorrected) && !f.cs3) &&
+      !(f.mtf_file != f.mtf_resolution) && (f.scherzer_defocus || f.defocus) &&
+      (f.scherzer_alphamax || f.alpha_max) &&
+      !((f.lammps_preTEM_file != f.lammps_TEM_steps) || (f.lammps_preTEM_file != f.lammps_TEM_samples));
+  if (!ok) {
+    j->messages += j->program + " : lacking required parameters\n";
+    if (!(f.scherzer_defocus || f.defocus))
+      j->messages += "You must specify either --defocus <value [angstrom]> or --scherzer_defocus\n";
+    if (!(f.scherzer_alphamax || f.alpha_max))
+      j->messages += "You must specify either --alphamax <value [radians]> or --scherzer_alphamax\n";
+    if ((f.adfstem_uncorrected || f.bfctem_uncorrected) && !f.cs3)
+      j->messages += "You must specify --cs3 when not using aberration correction\n";
+    if ((f.adfstem_corrected || f.bfctem_corrected) && !((f.cs3 || f.scherzer_cs3) && f.cs5))
+      j->messages += "Aberration correction requires --cs5 and either --cs3 or --scherzer_cs3\n";
+    f.fail = 1;
+  }
+  if (f.fail == 0 && !f.adfstem_uncorrected && !f.adfstem_corrected) {
+    j->messages += "Error: no simulation mode given (--adfstemuncorr, --adfstemcorr, "
+                   "--adfstemuncorrfem or --adfstemcorrfem)\n";
+    f.fail = 1;
+  }
+  if (f.adfstem_uncorrected && f.adfstem_corrected) {
+    j->messages += "Error: choose either aberration corrected or uncorrected modes\n";
+    f.fail = 1;
+  }
+  if (f.correlograph) {
+    j->messages += "Error, the correlograph outputs are not supported by this build\n";
+    f.fail = 1;
+  }
+  if (f.lammps_preTEM_file) {
+    j->messages += "Error, the LAMMPS-coupled FEM mode needs ms-stem-fem-md and LAMMPS, "
+                   "which are not available in this build\n";
+    f.fail = 1;
+  }
+}
+
+}  // namespace
+
+// read_position_lammps_data_file (tem_io.cpp:36-1028)
+msf_status read_lammps(const std::string& path, msf_job* j) {
+  std::ifstream in(path.c_str(), std::ifstream::in);
+  if (!in.is_open()) { j->messages += "Error opening position file\n"; return MSF_ERR_IO; }
+  auto fail = [&](const std::string& m) { j->messages += "Error reading position data file; " + m + "\n"; return MSF_ERR_PARSE; };
+  std::string line;
+  std::getline(in, line);  // first line is a comment
+  size_t declared = 0;
+  if (!next_line(in, line)) return fail("expected '<N> atoms'");
+  {
+    std::istringstream ls(line);
+    std::string d;
+    ls >> declared >> d;
+    if (!declared || lower(d) != "atoms") return fail("expected '<N> atoms'");
+  }
+  unsigned n_species = 0;
+  if (!next_line(in, line)) return fail("expected '<T> atom types'");
+  {
+    std::istringstream ls(line);
+    std::string d1, d2;
+    ls >> n_species >> d1 >> d2;
+    if (!n_species || lower(d1) != "atom" || lower(d2) != "types") return fail("expected '<T> atom types'");
+  }
+  double lo[3], hi[3];
+  const char* names[3][2] = {{"xlo", "xhi"}, {"ylo", "yhi"}, {"zlo", "zhi"}};
+  for (int d = 0; d < 3; ++d) {
+    if (!next_line(in, line)) return fail("expected box bounds");
+    std::istringstream ls(line);
+    std::string d1, d2;
+    ls >> lo[d] >> hi[d] >> d1 >> d2;
+    if (lower(d1) != names[d][0] || lower(d2) != names[d][1])
+      return fail(std::string("expected '<lo> <hi> ") + names[d][0] + " " + names[d][1] + "'");
+  }
+  for (int d = 0; d < 3; ++d)
+    if (hi[d] <= lo[d]) return fail("upper bound <= lower bound");
+  j->xperiod = hi[0] - lo[0];
+  j->yperiod = hi[1] - lo[1];
+  j->zperiod = hi[2] - lo[2];
+  if (!next_line(in, line)) return fail("expected 'Masses'");
+  {
+    std::istringstream ls(line);
+    std::string sec;
+    ls >> sec;
+    if (lower(sec) != "masses") return fail("expected 'Masses'");
+  }
+  std::vector<size_t> species_id(n_species, 0);
+  std::vector<double> masses(n_species, 0.0);
+  std::vector<unsigned> zs(n_species, 0);
+  for (unsigned k = 0; k < n_species && in.good(); ++k) {
+    if (next_line(in, line)) {
+      std::istringstream ls(line);
+      ls >> species_id[k] >> masses[k];
+    }
+  }
+  for (unsigned k = 0; k < n_species; ++k) {
+    zs[k] = msf::guess_z(masses[k]);
+    if (!zs[k]) {
+      j->messages += "Error: could not guess element having mass " + std::to_string(masses[k]) + "\n";
+      return MSF_ERR_PARSE;
+    }
+  }
+  if (!next_line(in, line)) return fail("expected 'Atoms'");
+  {
+    std::istringstream ls(line);
+    std::string sec;
+    ls >> sec;
+    if (lower(sec) != "atoms") return fail("expected 'Atoms'");
+  }
+  j->q.clear();
+  j->z.clear();
+  std::vector<size_t> types;
+  for (size_t read = 0; read < declared; ++read) {
+    if (!next_line(in, line)) return fail("fewer atoms than declared");
+    std::istringstream ls(line);
+    size_t id = 0, type = 0;
+    double p[3] = {0, 0, 0};
+    ls >> id >> type >> p[0] >> p[1] >> p[2];
+    size_t k = 0;
+    for (; k < n_species; ++k)
+      if (type == species_id[k]) break;
+    if (k >= n_species) return fail("atom type not declared in Masses");
+    if (id > declared || p[0] > hi[0] || p[0] < lo[0] || p[1] > hi[1] || p[1] < lo[1] ||
+        p[2] > hi[2] || p[2] < lo[2])
+      return fail("atom id or position outside the declared box");
+    for (int d = 0; d < 3; ++d) j->q.push_back(p[d]);
+    j->z.push_back(zs[k]);
+    types.push_back(type);
+  }
+  std::vector<size_t> uniq(types);
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  if (uniq.size() != n_species) return fail("number of atom types used differs from declared");
+  for (size_t a = 0; a < j->z.size(); ++a) {  // tem_io.cpp:907-916
+    j->q[3 * a] = j->q[3 * a] - lo[0];
+    j->q[3 * a + 1] = j->q[3 * a + 1] - lo[1];
+    j->q[3 * a + 2] = j->q[3 * a + 2] - lo[2];
+  }
+  j->xmin = j->ymin = j->zmin = 0.0;
+  return MSF_OK;
+}
+
+namespace {
+
+// tem.cpp:405-1378 after the inputs are read
+msf_status finish_job(msf_job* j) {
+  Flags& f = j->flags;
+  msf::wavelength(j->VV, &j->lambda, &j->gamma);
+  const double xpd = j->xperiod * j->dupe_x, ypd = j->yperiod * j->dupe_y;
+  double bw_pap = (j->nx / (2 * xpd) < j->ny / (2 * ypd)) ? j->nx / (2 * xpd) : j->ny / (2 * ypd);
+  double bw_t = (2.0 / 3.0) * bw_pap;
+  if ((f.adfstem_corrected || f.adfstem_uncorrected) && f.adfstem_detector_angles) {
+    if (j->det_inner < 0.0) { j->messages += "Error: detector_inner_angle < 0\n"; f.fail = 1; }
+    if (j->det_outer < 0.0) { j->messages += "Error: detector_outer_angle < 0\n"; f.fail = 1; }
+    if (j->det_inner > bw_t * j->lambda) {
+      j->messages += "Error: detector inner angle falls beyond bandwidth limits\n";
+      f.fail = 1;
+    }
+  }
+  if (f.fail) return MSF_ERR_ARG;
+  if (!f.adfstem_detector_angles) {  // tem.cpp:1320-1337
+    if (j->VV >= 200000) { j->det_inner = 0.040; j->det_outer = 0.200; }
+    else { j->det_inner = 0.045; j->det_outer = 0.200; }
+  }
+  if (!f.raster_spacing) j->raster_spacing = f.fem ? 10 : 1.5;  // tem.cpp:1342-1348
+  j->x_p = msf::raster_points(j->xperiod, j->xmin, j->raster_spacing);
+  j->y_p = msf::raster_points(j->yperiod, j->ymin, j->raster_spacing);
+  if (f.adfstem_uncorrected) {  // tem.cpp:1526-1558
+    if (f.scherzer_defocus) j->defocus = msf::scherzer(0, j->lambda, j->Cs3);
+    if (f.scherzer_alphamax) j->alpha_max = msf::scherzer(1, j->lambda, j->Cs3);
+    j->corrected = false;
+    j->cs3_used = j->Cs3;
+    j->full_prefix = j->output_prefix + "_adfstem_uncorr";
+  } else {  // tem.cpp:1565-1639
+    if (f.scherzer_defocus) j->defocus = msf::scherzer(2, j->lambda, j->Cs5);
+    if (f.scherzer_alphamax) j->alpha_max = msf::scherzer(3, j->lambda, j->Cs5);
+    j->cs3_used = f.scherzer_cs3 ? msf::scherzer(4, j->lambda, j->Cs5) : j->Cs3;
+    j->corrected = true;
+    j->full_prefix = j->output_prefix + "_adfstem_corr";
+  }
+  return MSF_OK;
+}
+
+// write_tif_grayscale<uint16_t> (write_tif.hpp:143-335): min/max scaled or
+// log-scaled 16-bit samples, rows written bottom-up, baseline tags.
+bool write_tif16(const std::string& name, const double* data, size_t height, size_t width,
+                 double mn, double mx, bool logscale, double xres, double yres,
+                 unsigned short res_unit) {
+  std::vector<uint16_t> img(width * height);
+  const double digits = std::pow(2, 16) - 1;
+  if (logscale) {
+    const double dl = std::log(mx - mn + 1);
+    for (size_t i = 0; i < height; ++i)
+      for (size_t k = 0; k < width; ++k) {
+        const double v = std::log(data[k + width * i] - mn + 1) / dl;
+        img[k + width * i] = v > 0.0 ? (uint16_t)(v * digits + 0.5) : (uint16_t)0;
+      }
+  } else {
+    const double sc = digits / (mx - mn);
+    for (size_t i = 0; i < height; ++i)
+      for (size_t k = 0; k < width; ++k)
+        img[k + width * i] = (uint16_t)((data[k + width * i] - mn) * sc + 0.5);
+  }
+  std::vector<unsigned char> out;
+  auto p16 = [&](unsigned v) { out.push_back(v & 0xff); out.push_back((v >> 8) & 0xff); };
+  auto p32 = [&](unsigned v) { for (int b = 0; b < 4; ++b) out.push_back((v >> (8 * b)) & 0xff); };
+  out.push_back('I'); out.push_back('I'); p16(42); p32(0);
+  const uint32_t rps = (uint32_t)width;  // TIFFDefaultStripSize(width) = width
+  const size_t line = width * 2;
+  std::vector<uint32_t> offs, counts;
+  for (size_t r0 = 0; r0 < height; r0 += rps) {
+    const size_t r1 = std::min(height, r0 + rps);
+    offs.push_back((uint32_t)out.size());
+    counts.push_back((uint32_t)((r1 - r0) * line));
+    for (size_t r = r0; r < r1; ++r) {
+      const uint16_t* src = &img[(height - r - 1) * width];
+      for (size_t k = 0; k < width; ++k) p16(src[k]);
+    }
+  }
+  if (out.size() & 1) out.push_back(0);
+  const uint32_t den = 10000;
+  const uint32_t xoff = (uint32_t)out.size();
+  p32((uint32_t)std::llround(xres * den)); p32(den);
+  const uint32_t yoff = (uint32_t)out.size();
+  p32((uint32_t)std::llround(yres * den)); p32(den);
+  uint32_t soff = 0, coff = 0;
+  if (offs.size() > 1) {
+    soff = (uint32_t)out.size();
+    for (uint32_t v : offs) p32(v);
+    coff = (uint32_t)out.size();
+    for (uint32_t v : counts) p32(v);
+  }
+  struct E { unsigned tag, type, count, value; };
+  const unsigned ns = (unsigned)offs.size();
+  std::vector<E> es = {{256, 4, 1, (unsigned)width},  {257, 4, 1, (unsigned)height},
+                       {258, 3, 1, 16},               {259, 3, 1, 1},
+                       {262, 3, 1, 1},                {273, 4, ns, ns > 1 ? soff : offs[0]},
+                       {274, 3, 1, 1},                {277, 3, 1, 1},
+                       {278, 4, 1, rps},              {279, 4, ns, ns > 1 ? coff : counts[0]},
+                       {282, 5, 1, xoff},             {283, 5, 1, yoff},
+                       {284, 3, 1, 1},                {296, 3, 1, res_unit}};
+  const uint32_t ifd = (uint32_t)out.size();
+  for (int b = 0; b < 4; ++b) out[4 + b] = (ifd >> (8 * b)) & 0xff;
+  p16((unsigned)es.size());
+  for (const E& e : es) {
+    p16(e.tag); p16(e.type); p32(e.count);
+    if (e.type == 3 && e.count == 1) { p16(e.value); p16(0); } else p32(e.value);
+  }
+  p32(0);
+  FILE* fp = std::fopen(name.c_str(), "wb");
+  if (!fp) return false;
+  const bool ok = std::fwrite(out.data(), 1, out.size(), fp) == out.size();
+  std::fclose(fp);
+  return ok;
+}
+
+bool write_variance(const std::string& prefix, const double* k_lower, const double* v, int n) {
+  FILE* fp = std::fopen((prefix + ".txt").c_str(), "w");
+  if (!fp) return false;
+  for (int i = 0; i < n; ++i) std::fprintf(fp, "%.10e %.10e\n", k_lower[i], v[i]);
+  std::fclose(fp);
+  return true;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- C ABI ------
+extern "C" {
+
+msf_status msf_read_specimen(const char* path, msf_job** out) {
+  if (!path || !out) return MSF_ERR_ARG;
+  msf_job* j = new msf_job;
+  const std::string p(path);
+  msf_status st;
+  if (p.size() > 4 && p.substr(p.find_last_of('.') + 1) == "xyz") {
+    j->messages += "Error, xyz specimen files are not supported by this build\n";
+    st = MSF_ERR_UNSUPPORTED;
+  } else {
+    st = read_lammps(p, j);
+  }
+  if (st != MSF_OK) {
+    msf::set_error(j->messages);
+    delete j;
+    return st;
+  }
+  *out = j;
+  return MSF_OK;
+}
+
+msf_status msf_parse_cmdline(int32_t argc, const char* const* argv, msf_job** out) {
+  if (!out || argc < 1 || !argv) return MSF_ERR_ARG;
+  msf_job* j = new msf_job;
+  std::vector<std::string> args(argv, argv + argc);
+  j->program = args[0];
+  parse_args(args, j);
+  // tem.cpp:240-330: the specimen is read before the flag checks
+  msf_status st = MSF_OK;
+  if (!j->model_file.empty() &&
+      j->model_file.substr(j->model_file.find_last_of('.') + 1) == "xyz") {
+    j->messages += "Error, xyz specimen files are not supported by this build\n";
+    j->flags.fail = 1;
+    st = MSF_ERR_UNSUPPORTED;
+  } else if (read_lammps(j->model_file, j) != MSF_OK) {
+    j->messages += "Error, file could not be read : " + j->model_file + "\n";
+    j->flags.fail = 1;
+    st = MSF_ERR_IO;
+  }
+  check_flags(j);
+  if (j->flags.fail) {
+    msf::set_error(j->messages + "Exiting ms-stem-fem due to failure.\n");
+    delete j;
+    return st != MSF_OK ? st : MSF_ERR_PARSE;
+  }
+  st = finish_job(j);
+  if (st != MSF_OK) {
+    msf::set_error(j->messages);
+    delete j;
+    return st;
+  }
+  *out = j;
+  return MSF_OK;
+}
+
+msf_status msf_job_destroy(msf_job* job) {
+  delete job;
+  return MSF_OK;
+}
+
+msf_status msf_job_describe(const msf_job* j, msf_grid* grid, msf_atoms* atoms,
+                            msf_optics* optics, msf_raster* raster, msf_detect* det) {
+  if (!j) return MSF_ERR_ARG;
+  const Flags& f = j->flags;
+  if (grid) {
+    *grid = msf_grid{};
+    grid->nx = j->nx;
+    grid->ny = j->ny;
+    grid->voltage = j->VV;
+    grid->xperiod = j->xperiod;
+    grid->yperiod = j->yperiod;
+    grid->zperiod = j->zperiod;
+    grid->dupe_x = (int32_t)j->dupe_x;
+    grid->dupe_y = (int32_t)j->dupe_y;
+    grid->dupe_z = (int32_t)j->dupe_z;
+    // tem.cpp:1051-1058
+    grid->replicate_atoms = (f.dupe && f.fem && (j->dupe_x > 1 || j->dupe_y > 1 || j->dupe_z > 1) &&
+                             (j->dupe_x > 0 && j->dupe_y > 0 && j->dupe_z > 0)) ? 1 : 0;
+    grid->xmin = j->xmin;
+    grid->ymin = j->ymin;
+    grid->zmin = j->zmin;
+    grid->min_slice = j->min_slice;
+  }
+  if (atoms) {
+    atoms->n_atoms = (int64_t)j->z.size();
+    atoms->q = j->q.data();
+    atoms->z = j->z.data();
+  }
+  if (optics) {
+    optics->corrected = j->corrected ? 1 : 0;
+    optics->cs3 = j->cs3_used;
+    optics->cs5 = j->Cs5;
+    optics->defocus = j->defocus;
+    optics->alpha_max = j->alpha_max;
+  }
+  if (raster) {
+    raster->n_x = (int32_t)j->x_p.size();
+    raster->n_y = (int32_t)j->y_p.size();
+    raster->x_p = j->x_p.data();
+    raster->y_p = j->y_p.data();
+  }
+  if (det) {
+    det->outputs = 0;
+    if (f.image_output) det->outputs |= MSF_OUT_ADF_IMAGE;
+    if (f.fem) {
+      if (f.d1) det->outputs |= MSF_OUT_V_OMEGA;
+      if (f.d2) det->outputs |= MSF_OUT_VBAR_R;
+      if (f.d3) det->outputs |= MSF_OUT_V_RE;
+      if (f.d4) det->outputs |= MSF_OUT_OMEGA_VIMAGE;
+      if (f.gt17) det->outputs |= MSF_OUT_V_GT17;
+      if (f.rva) det->outputs |= MSF_OUT_V_RBAR;
+    }
+    det->det_inner = j->det_inner;
+    det->det_outer = j->det_outer;
+    det->dr = j->dr;
+  }
+  return MSF_OK;
+}
+
+const char* msf_job_output_prefix(const msf_job* j) { return j ? j->full_prefix.c_str() : ""; }
+
+msf_status msf_write_outputs(const msf_job* j, const msf_results* r) {
+  if (!j || !r) return MSF_ERR_ARG;
+  const Flags& f = j->flags;
+  const std::string& pre = j->full_prefix;
+  if (f.fem && r->k_lower) {
+    struct M { unsigned on; const double* v; const char* name; };
+    const M modes[] = {{f.d1, r->v_omega, "_fem_V_omega"},   {f.d2, r->vbar_r, "_fem_Vbar_r"},
+                       {f.gt17, r->v_gt17, "_fem_V_gt17"},   {f.d3, r->v_re, "_fem_V_re"},
+                       {f.rva, r->v_rbar, "_fem_V_rbar"},    {f.d4, r->omega_vimage, "_fem_Omega_vimage"}};
+    for (const M& m : modes)
+      if (m.on && m.v && !write_variance(pre + m.name, r->k_lower, m.v, r->n_k)) {
+        msf::set_error("Unable to write variance to file: " + pre + m.name + ".txt");
+        return MSF_ERR_IO;
+      }
+  }
+  if (f.image_output && r->adf_image) {
+    const size_t nx = j->x_p.size(), ny = j->y_p.size();
+    const double* img = r->adf_image;
+    double mn = img[0], mx = img[0];
+    for (size_t k = 0; k < nx * ny; ++k) { mx = std::max(mx, img[k]); mn = std::min(mn, img[k]); }
+    const double xres = (nx / j->xperiod) * 1.0e8, yres = (ny / j->yperiod) * 1.0e8;
+    const std::string base = pre + "_stem_image_output";
+    if (!write_tif16(base + ".tif", img, nx, ny, mn, mx, false, xres, yres, 3) ||
+        !write_tif16(base + "_logscale.tif", img, nx, ny, mn, mx, true, xres, yres, 3)) {
+      msf::set_error("could not write " + base + ".tif");
+      return MSF_ERR_IO;
+    }
+    FILE* fp = std::fopen((base + ".f64").c_str(), "wb");
+    if (fp) { std::fwrite(img, sizeof(double), nx * ny, fp); std::fclose(fp); }
+  }
+  return MSF_OK;
+}
+
+int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) {
+  msf_job* j = nullptr;
+  msf_status st = msf_parse_cmdline(argc, argv, &j);
+  if (st != MSF_OK) {
+    std::cout << msf::last_error();
+    return 1;
+  }
+  msf_options o{};
+  o.precision = MSF_FP64;
+  o.use_graphs = 1;
+  if (opt) o = *opt;
+  msf_context* ctx = nullptr;
+  msf_specimen* spec = nullptr;
+  msf_grid grid;
+  msf_atoms atoms;
+  msf_optics optics;
+  msf_raster raster;
+  msf_detect det;
+  msf_job_describe(j, &grid, &atoms, &optics, &raster, &det);
+  int rc = 1;
+  if ((st = msf_context_create(&o, &ctx)) == MSF_OK &&
+      (st = msf_specimen_create(ctx, &grid, &atoms, &spec)) == MSF_OK) {
+    const size_t nr = raster.n_x * (size_t)raster.n_y;
+    std::vector<double> img(nr), kl(8192), v[6];
+    for (auto& a : v) a.assign(8192, 0.0);
+    msf_results r{};
+    r.adf_image = img.data();
+    r.cap_k = 8192;
+    r.k_lower = kl.data();
+    r.v_omega = v[0].data();
+    r.vbar_r = v[1].data();
+    r.v_re = v[2].data();
+    r.omega_vimage = v[3].data();
+    r.v_gt17 = v[4].data();
+    r.v_rbar = v[5].data();
+    if ((st = msf_run(ctx, spec, &optics, &raster, &det, &r)) == MSF_OK &&
+        (st = msf_write_outputs(j, &r)) == MSF_OK)
+      rc = 0;
+  }
+  if (rc != 0) std::cerr << "ms-stem-fem: " << msf::last_error() << std::endl;
+  msf_specimen_destroy(spec);
+  msf_context_destroy(ctx);
+  msf_job_destroy(j);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,558 @@
+// sm_100a kernels of the multislice path.
+//
+// Wavefield layout in HBM: [probe][x][y] complex (float2 / double2), y
+// fastest, as the reference's fftw_complex psi[j + i*Ny] (adfstem.cpp:1665)
+// with one contiguous nx*ny plane per probe of the batch.
+//
+// Per slice the two fused passes are
+//   row pass    (contiguous, along y):  iDFT_y, t * psi / s (quirk kept),
+//                                       DFT_y                  [ROW_SLICE]
+//   column pass (strided,   along x):   DFT_x, / s, band-limit mask,
+//                                       propagator, iDFT_x     [COL_SLICE]
+// which together equal the reference's iFFT2 -> *t -> FFT2 -> bw_limit ->
+// propagate (adfstem.cpp:1891-2048).  The first slice's row pass reads the
+// shifted probe directly (ROW_SLICE_FIRST, adfstem.cpp:1632-1837) and the
+// last slice's column pass stops in k-space for detection (COL_SLICE_LAST).
+#include "kernels.h"
+#include "fft_core.cuh"
+
+#include <cmath>
+#include <cstdio>
+
+namespace msf {
+
+namespace {
+
+constexpr double kRefPi = 3.14159265369;  // the reference's PI (adfstem.hpp:55)
+constexpr int kSmemBudget = 220 * 1024;
+
+template <typename Real, int N>
+constexpr int row_lines() {
+  using Sh = Shape<N, Real>;
+  constexpr int bytes = Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  int l = 256 / Sh::T;
+  if (l < 1) l = 1;
+  while (l > 1 && l * bytes > kSmemBudget) l >>= 1;
+  return l;
+}
+
+template <typename Real, int N>
+constexpr int col_cols() {
+  using Sh = Shape<N, Real>;
+  constexpr int bytes = Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  int c = sizeof(Real) == 4 ? 16 : 8;
+  while (c > 1 && (c * bytes > kSmemBudget || c * Sh::T > 256)) c >>= 1;
+  return c;
+}
+
+// ------------------------------------------------------------ row pass ---
+template <typename Real, int N, int LINES, int OP>
+__global__ void __launch_bounds__(LINES * Shape<N, Real>::T)
+row_kernel(const PassArgs a) {
+  using C = Cx<Real>;
+  using Sh = Shape<N, Real>;
+  using SM = Smem<Sh>;
+  constexpr int E = Sh::E, T = Sh::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* smem = reinterpret_cast<C*>(smem_raw);
+  const int line = threadIdx.x / T;
+  const int t = threadIdx.x % T;
+  const int b = blockIdx.x;
+  const int i = blockIdx.y * LINES + line;
+  C* sm = smem + line * SM::stride;
+  C* row = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)i * N;
+  const C* tw = static_cast<const C*>(a.tw);
+  auto sync = [] {
+    if constexpr (T <= 32) __syncwarp();
+    else __syncthreads();
+  };
+  C v[E];
+  if constexpr (OP == ROW_SLICE_FIRST) {
+    const int sx = a.shifts[2 * b], sy = a.shifts[2 * b + 1];
+    const int ix = (i < sx) ? i + a.nx - sx : i - sx;
+    const C* prow = static_cast<const C*>(a.probe) + (int64_t)ix * N;
+    const Real fs = (Real)a.first_scale;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int y = t + T * m;
+      const int iy = (y < sy) ? y + N - sy : y - sy;
+      v[m] = cscale(__ldg(prow + iy), fs);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = row[t + T * m];
+  }
+  if constexpr (OP == ROW_FWD) {
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+  } else if constexpr (OP == ROW_INV) {
+    fft_line<Sh, true>(v, sm, t, tw, sync);
+    const Real s = (Real)a.scale;
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = cscale(v[m], s);
+  } else {
+    if constexpr (OP == ROW_SLICE) fft_line<Sh, true>(v, sm, t, tw, sync);
+    // transmission multiply with the reference's in-place update order
+    // (adfstem.cpp:1929-1949): the new real part feeds the imaginary part.
+    const C* trow = static_cast<const C*>(a.trans) + (int64_t)i * N;
+    const Real is = (Real)a.inv_s;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const C tv = __ldg(trow + t + T * m);
+      const Real re = (tv.x * v[m].x - tv.y * v[m].y) * is;
+      const Real im = (tv.x * v[m].y + tv.y * re) * is;
+      v[m] = C{re, im};
+    }
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+  }
+#pragma unroll
+  for (int m = 0; m < E; ++m) row[t + T * m] = v[m];
+}
+
+// --------------------------------------------------------- column pass ---
+template <typename Real, int N, int COLS, int OP>
+__global__ void __launch_bounds__(COLS * Shape<N, Real>::T)
+col_kernel(const PassArgs a) {
+  using C = Cx<Real>;
+  using Sh = Shape<N, Real>;
+  using SM = Smem<Sh>;
+  constexpr int E = Sh::E, T = Sh::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* smem = reinterpret_cast<C*>(smem_raw);
+  const int c = threadIdx.x % COLS;
+  const int t = threadIdx.x / COLS;
+  const int b = blockIdx.x;
+  const int j = blockIdx.y * COLS + c;
+  const int64_t ny = a.ny;
+  C* col = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + j;
+  C* sm = smem + c * SM::stride;
+  const C* tw = static_cast<const C*>(a.tw);
+  auto sync = [] { __syncthreads(); };
+  C v[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) v[m] = col[(int64_t)(t + T * m) * ny];
+  if constexpr (OP == COL_INV) {
+    fft_line<Sh, true>(v, sm, t, tw, sync);
+    const Real s = (Real)a.scale;
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = cscale(v[m], s);
+  } else {
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+    if constexpr (OP != COL_FWD) {
+      const int lo = __ldg(a.mask_lo + j), hi = __ldg(a.mask_hi + j);
+      if constexpr (OP == COL_FWD_MASK_INV) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const int i = t + T * m;
+          if (!(i < lo || i >= hi)) v[m] = C{(Real)0, (Real)0};
+        }
+      } else {
+        const Real is = (Real)a.inv_s;
+        const C pyj = __ldg(static_cast<const C*>(a.py) + j);
+        const C* px = static_cast<const C*>(a.px);
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const int i = t + T * m;
+          if (i < lo || i >= hi) {
+            const C p = cmul(__ldg(px + i), pyj);  // slice.cpp:1396-1412
+            v[m] = cmul(p, cscale(v[m], is));
+          } else {
+            v[m] = C{(Real)0, (Real)0};
+          }
+        }
+      }
+      if constexpr (OP == COL_FWD_MASK_INV || OP == COL_SLICE)
+        fft_line<Sh, true>(v, sm, t, tw, sync);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < E; ++m) col[(int64_t)(t + T * m) * ny] = v[m];
+}
+
+template <typename Real, int N, int OP>
+cudaError_t row_launch(const PassArgs& a, cudaStream_t s) {
+  constexpr int L = row_lines<Real, N>();
+  using Sh = Shape<N, Real>;
+  constexpr int smem = L * Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  static bool configured = false;
+  auto k = row_kernel<Real, N, L, OP>;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  if (a.nx % L != 0) return cudaErrorInvalidValue;
+  dim3 grid(a.nb, a.nx / L);
+  k<<<grid, L * Sh::T, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename Real, int N, int OP>
+cudaError_t col_launch(const PassArgs& a, cudaStream_t s) {
+  constexpr int CC = col_cols<Real, N>();
+  using Sh = Shape<N, Real>;
+  constexpr int smem = CC * Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  static bool configured = false;
+  auto k = col_kernel<Real, N, CC, OP>;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  if (a.ny % CC != 0) return cudaErrorInvalidValue;
+  dim3 grid(a.nb, a.ny / CC);
+  k<<<grid, CC * Sh::T, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename Real, int OP>
+cudaError_t row_dispatch(const PassArgs& a, cudaStream_t s) {
+  switch (a.ny) {
+    case 64: return row_launch<Real, 64, OP>(a, s);
+    case 128: return row_launch<Real, 128, OP>(a, s);
+    case 256: return row_launch<Real, 256, OP>(a, s);
+    case 512: return row_launch<Real, 512, OP>(a, s);
+    case 1024: return row_launch<Real, 1024, OP>(a, s);
+    case 2048: return row_launch<Real, 2048, OP>(a, s);
+    case 4096: return row_launch<Real, 4096, OP>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename Real, int OP>
+cudaError_t col_dispatch(const PassArgs& a, cudaStream_t s) {
+  switch (a.nx) {
+    case 64: return col_launch<Real, 64, OP>(a, s);
+    case 128: return col_launch<Real, 128, OP>(a, s);
+    case 256: return col_launch<Real, 256, OP>(a, s);
+    case 512: return col_launch<Real, 512, OP>(a, s);
+    case 1024: return col_launch<Real, 1024, OP>(a, s);
+    case 2048: return col_launch<Real, 2048, OP>(a, s);
+    case 4096: return col_launch<Real, 4096, OP>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------ set-up kernels ---
+__device__ __forceinline__ double ksq_exact(double kx, double ky) {
+  // pow(kx,2) + pow(ky,2) / kx*kx + ky*ky without contraction
+  return __dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky));
+}
+
+__global__ void lut_synth_kernel(double2* out, const double* __restrict__ kx,
+                                 const double* __restrict__ ky, int nx, int ny,
+                                 const double* __restrict__ p, double pref,
+                                 double cutoff_sq, double xmin, double ymin) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)nx * ny) return;
+  const int i = (int)(idx / ny), j = (int)(idx % ny);
+  const double kxi = kx[i], kyj = ky[j];
+  const double ksq = ksq_exact(kxi, kyj);
+  double2 r = make_double2(0.0, 0.0);
+  if (ksq < cutoff_sq) {
+    // f_ej_single_scatterer (projected_atomic_potential.cpp:209-220)
+    const double f = p[0] / (ksq + p[3]) + p[1] / (ksq + p[4]) + p[2] / (ksq + p[5]) +
+                     p[6] * exp(-p[9] * ksq) + p[7] * exp(-p[10] * ksq) +
+                     p[8] * exp(-p[11] * ksq);
+    const double trig = 2 * kRefPi * (kxi * xmin + kyj * ymin);
+    double sn, cs;
+    sincos(trig, &sn, &cs);
+    r.x = pref * f * cs;
+    r.y = pref * f * sn;
+  }
+  out[idx] = r;
+}
+
+constexpr int kPotRows = 4;
+constexpr int kPotChunk = 512;
+
+// Each CTA owns a kPotRows x blockDim.x tile of the slice's potential and
+// accumulates it in registers over the slice's atoms (staged in shared
+// memory in chunks), in the reference's atom order so the FP64 sums equal
+// slice.cpp:1594-1649 term for term.  The LUT spans the whole cell, so every
+// atom contributes to every tile; no global atomics are used.
+__global__ void potential_kernel(double2* __restrict__ t, const double2* __restrict__ luts,
+                                 int nx, int ny, const int32_t* __restrict__ asx,
+                                 const int32_t* __restrict__ asy,
+                                 const int32_t* __restrict__ asp, int n_atoms) {
+  __shared__ int3 atoms[kPotChunk];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = blockIdx.y * kPotRows;
+  const int64_t plane = (int64_t)nx * ny;
+  double2 acc[kPotRows];
+#pragma unroll
+  for (int r = 0; r < kPotRows; ++r) acc[r] = make_double2(0.0, 0.0);
+  for (int c0 = 0; c0 < n_atoms; c0 += kPotChunk) {
+    const int cn = min(kPotChunk, n_atoms - c0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < cn; k += blockDim.x)
+      atoms[k] = make_int3(asx[c0 + k], asy[c0 + k], asp[c0 + k]);
+    __syncthreads();
+    if (j < ny) {
+      for (int k = 0; k < cn; ++k) {
+        const int3 a = atoms[k];
+        const double2* lut = luts + (int64_t)a.z * plane;
+        const int jy = (j < a.y) ? j + ny - a.y : j - a.y;
+#pragma unroll
+        for (int r = 0; r < kPotRows; ++r) {
+          const int i = i0 + r;
+          const int ix = (i < a.x) ? i + nx - a.x : i - a.x;
+          const double2 l = __ldg(lut + (int64_t)ix * ny + jy);
+          acc[r].x = __dadd_rn(acc[r].x, l.x);
+          acc[r].y = __dadd_rn(acc[r].y, l.y);
+        }
+      }
+    }
+  }
+  if (j < ny) {
+#pragma unroll
+    for (int r = 0; r < kPotRows; ++r) {
+      // slice.cpp:1700-1725
+      const double e = exp(-(acc[r].y));
+      double sn, cs;
+      sincos(acc[r].x, &sn, &cs);
+      t[(int64_t)(i0 + r) * ny + j] = make_double2(e * cs, e * sn);
+    }
+  }
+}
+
+__global__ void probe_synth_kernel(double2* out, const double* __restrict__ kx,
+                                   const double* __restrict__ ky, int nx, int ny,
+                                   int corrected, double cs3, double cs5,
+                                   double defocus, double lambda, double lsq,
+                                   double amax_sq, double x0, double y0) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)nx * ny) return;
+  const int i = (int)(idx / ny), j = (int)(idx % ny);
+  const double kxi = kx[i], kyj = ky[j];
+  const double ksqr = ksq_exact(kxi, kyj);
+  double2 r = make_double2(0.0, 0.0);
+  if (__dmul_rn(lsq, ksqr) < amax_sq) {  // probe_wavefunction.cpp:100
+    double chi;
+    if (corrected) {  // lenses.cpp:263-290
+      const double kl = ksqr * lsq;
+      chi = kRefPi * lambda * ksqr * (-defocus + 0.5 * cs3 * kl + (1.0 / 3.0) * cs5 * (kl * kl));
+    } else {  // lenses.cpp:249-261
+      chi = kRefPi * lambda * ksqr * (0.5 * cs3 * lsq * ksqr - defocus);
+    }
+    const double trig = chi + 2 * kRefPi * ((kxi * x0) + (kyj * y0));
+    double sn, cs;
+    sincos(trig, &sn, &cs);
+    r = make_double2(cs, -1.0 * sn);
+  }
+  out[idx] = r;
+}
+
+__global__ void norm2_kernel(const double2* __restrict__ a, int64_t n, double* out) {
+  __shared__ double red[1024];
+  double s = 0.0;
+  for (int64_t k = threadIdx.x; k < n; k += blockDim.x) {
+    const double2 v = a[k];
+    s += v.x * v.x + v.y * v.y;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0];
+}
+
+__global__ void scale_kernel(double2* a, int64_t n, double s) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) a[k] = make_double2(a[k].x * s, a[k].y * s);
+}
+
+__global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__ out,
+                              int64_t n) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = (float)in[k];
+}
+
+// ------------------------------------------------------- detection -------
+template <typename Real>
+__global__ void segment_sums_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
+                                    const int32_t* __restrict__ idx,
+                                    const int32_t* __restrict__ start, int ng,
+                                    double* amp, double* inten) {
+  __shared__ double ra[32], ri[32];
+  const int g = blockIdx.x, b = blockIdx.y;
+  const Cx<Real>* p = psi + (int64_t)b * stride;
+  double sa = 0.0, si = 0.0;
+  const int s0 = start[g], s1 = start[g + 1];
+  for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
+    const Cx<Real> v = p[idx[k]];
+    const double x = (double)v.x, y = (double)v.y;
+    const double i2 = x * x + y * y;
+    si += i2;
+    sa += sqrt(i2);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sa += __shfl_down_sync(0xffffffffu, sa, o);
+    si += __shfl_down_sync(0xffffffffu, si, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { ra[w] = sa; ri[w] = si; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    sa = l < nw ? ra[l] : 0.0;
+    si = l < nw ? ri[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sa += __shfl_down_sync(0xffffffffu, sa, o);
+      si += __shfl_down_sync(0xffffffffu, si, o);
+    }
+    if (l == 0) {
+      if (amp) amp[(int64_t)b * ng + g] = sa;
+      if (inten) inten[(int64_t)b * ng + g] = si;
+    }
+  }
+}
+
+template <typename Real>
+__global__ void pixel_accum_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
+                                   int nb, int64_t npix, double* acc_a, double* acc_i) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix) return;
+  double sa = acc_a[p], si = acc_i[p];
+  for (int b = 0; b < nb; ++b) {
+    const Cx<Real> v = psi[(int64_t)b * stride + p];
+    const double x = (double)v.x, y = (double)v.y;
+    const double i2 = x * x + y * y;
+    sa += sqrt(i2);
+    si += i2;
+  }
+  acc_a[p] = sa;
+  acc_i[p] = si;
+}
+
+inline unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
+
+}  // namespace
+
+bool supported_length(int n) {
+  return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096;
+}
+
+cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s) {
+  if (fp64) {
+    switch (op) {
+      case ROW_FWD: return row_dispatch<double, ROW_FWD>(a, s);
+      case ROW_INV: return row_dispatch<double, ROW_INV>(a, s);
+      case ROW_SLICE: return row_dispatch<double, ROW_SLICE>(a, s);
+      case ROW_SLICE_FIRST: return row_dispatch<double, ROW_SLICE_FIRST>(a, s);
+    }
+  } else {
+    switch (op) {
+      case ROW_SLICE: return row_dispatch<float, ROW_SLICE>(a, s);
+      case ROW_SLICE_FIRST: return row_dispatch<float, ROW_SLICE_FIRST>(a, s);
+      default: return cudaErrorInvalidValue;  // set-up transforms run in FP64
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s) {
+  if (fp64) {
+    switch (op) {
+      case COL_FWD: return col_dispatch<double, COL_FWD>(a, s);
+      case COL_INV: return col_dispatch<double, COL_INV>(a, s);
+      case COL_FWD_MASK_INV: return col_dispatch<double, COL_FWD_MASK_INV>(a, s);
+      case COL_SLICE: return col_dispatch<double, COL_SLICE>(a, s);
+      case COL_SLICE_LAST: return col_dispatch<double, COL_SLICE_LAST>(a, s);
+    }
+  } else {
+    switch (op) {
+      case COL_SLICE: return col_dispatch<float, COL_SLICE>(a, s);
+      case COL_SLICE_LAST: return col_dispatch<float, COL_SLICE_LAST>(a, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+void fill_twiddles(int n, double* h) {
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int m = 0; m < n; ++m) {
+    const double a = two_pi * (double)m / (double)n;
+    h[2 * m] = std::cos(a);
+    h[2 * m + 1] = -std::sin(a);
+  }
+}
+
+cudaError_t launch_lut_synth(double* out, const double* kx, const double* ky, int nx,
+                             int ny, const double* params12, double prefactor,
+                             double cutoff_sq, double xmin, double ymin, cudaStream_t s) {
+  const int64_t n = (int64_t)nx * ny;
+  lut_synth_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(out), kx, ky, nx, ny, params12, prefactor, cutoff_sq,
+      xmin, ymin);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_potential(double* t, const double* luts, int nx, int ny,
+                             const int32_t* asx, const int32_t* asy, const int32_t* asp,
+                             int n_atoms, cudaStream_t s) {
+  if (nx % kPotRows) return cudaErrorInvalidValue;
+  const int tpb = ny < 256 ? ny : 256;
+  dim3 grid((ny + tpb - 1) / tpb, nx / kPotRows);
+  potential_kernel<<<grid, tpb, 0, s>>>(reinterpret_cast<double2*>(t),
+                                        reinterpret_cast<const double2*>(luts), nx, ny,
+                                        asx, asy, asp, n_atoms);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_probe_synth(double* out, const double* kx, const double* ky, int nx,
+                               int ny, int corrected, double cs3, double cs5, double defocus,
+                               double lambda, double lambda_sq, double alpha_max_sq,
+                               double x0, double y0, cudaStream_t s) {
+  const int64_t n = (int64_t)nx * ny;
+  probe_synth_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(out), kx, ky, nx, ny, corrected, cs3, cs5, defocus, lambda,
+      lambda_sq, alpha_max_sq, x0, y0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_norm2(const double* a, int64_t n, double* out, cudaStream_t s) {
+  norm2_kernel<<<1, 1024, 0, s>>>(reinterpret_cast<const double2*>(a), n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(double* a, int64_t n, double sc, const double*, cudaStream_t s) {
+  scale_kernel<<<blocks_for(n, 256), 256, 0, s>>>(reinterpret_cast<double2*>(a), n, sc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t s) {
+  to_f32_kernel<<<blocks_for(n, 256), 256, 0, s>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t stride, int nb,
+                                const int32_t* idx, const int32_t* start, int ng,
+                                double* amp, double* inten, cudaStream_t s) {
+  if (ng <= 0 || nb <= 0) return cudaSuccess;
+  dim3 grid(ng, nb);
+  if (fp64)
+    segment_sums_kernel<double><<<grid, 256, 0, s>>>(
+        static_cast<const double2*>(psi), stride, idx, start, ng, amp, inten);
+  else
+    segment_sums_kernel<float><<<grid, 256, 0, s>>>(
+        static_cast<const float2*>(psi), stride, idx, start, ng, amp, inten);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t stride, int nb,
+                               int64_t npix, double* acc_a, double* acc_i, cudaStream_t s) {
+  if (fp64)
+    pixel_accum_kernel<double><<<blocks_for(npix, 256), 256, 0, s>>>(
+        static_cast<const double2*>(psi), stride, nb, npix, acc_a, acc_i);
+  else
+    pixel_accum_kernel<float><<<blocks_for(npix, 256), 256, 0, s>>>(
+        static_cast<const float2*>(psi), stride, nb, npix, acc_a, acc_i);
+  return cudaGetLastError();
+}
+
+}  // namespace msf

@@ -1,0 +1,91 @@
+// Host-callable launchers for the sm_100a kernels in kernels.cu.
+// No CUDA types beyond cudaStream_t cross this header; all device pointers
+// are passed as void* / typed raw pointers owned by the caller.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace msf {
+
+// Which fused operation a row pass (transform along y, contiguous) does.
+enum RowOp : int {
+  ROW_FWD = 0,          // forward DFT along y
+  ROW_INV = 1,          // inverse DFT along y, then * scale
+  ROW_SLICE = 2,        // inverse DFT, transmission multiply, forward DFT
+  ROW_SLICE_FIRST = 3,  // place shifted probe, transmission multiply, fwd DFT
+};
+// Which fused operation a column pass (transform along x, strided) does.
+enum ColOp : int {
+  COL_FWD = 0,           // forward DFT along x
+  COL_INV = 1,           // inverse DFT along x, then * scale
+  COL_FWD_MASK_INV = 2,  // forward DFT, band-limit mask, inverse DFT
+  COL_SLICE = 3,         // fwd DFT, /s, mask, propagator, inverse DFT
+  COL_SLICE_LAST = 4,    // fwd DFT, /s, mask, propagator (stay in k-space)
+};
+
+struct PassArgs {
+  void* psi = nullptr;            // [nb][nx][ny] complex (float2 or double2)
+  int64_t batch_stride = 0;       // elements between arrays
+  int nb = 1;                     // arrays in the batch
+  int nx = 0, ny = 0;
+  const void* tw = nullptr;       // twiddle table for the transformed length
+  // row slice ops
+  const void* trans = nullptr;    // [nx][ny] complex, this slice
+  double inv_s = 1.0;             // 1/sqrt(nx*ny)
+  const void* probe = nullptr;    // [nx][ny] complex, normalised real space
+  const int32_t* shifts = nullptr;// [nb][2] (sx, sy)
+  double first_scale = 1.0;       // nx*ny/s
+  double scale = 1.0;             // ROW_INV / COL_INV
+  // column mask and propagator
+  const int32_t* mask_lo = nullptr;  // [ny]: keep i < lo[j] || i >= hi[j]
+  const int32_t* mask_hi = nullptr;
+  const void* px = nullptr;       // [nx] complex propagator along x (Real2)
+  const void* py = nullptr;       // [ny] complex propagator along y (Real2)
+};
+
+// Returns false if the length is not supported.
+bool supported_length(int n);
+cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s);
+cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s);
+
+// Twiddle table e^{-2 pi i m / n}, m < n, computed in FP64 on the host.
+void fill_twiddles(int n, double* host_interleaved /* 2n */);
+
+// ---- set-up kernels (FP64) ----
+// sigma*V_z(k) of one species in k-space (scatterer_pap.hpp:109-151).
+cudaError_t launch_lut_synth(double* out, const double* kx, const double* ky,
+                             int nx, int ny, const double* params12,
+                             double prefactor, double cutoff_sq, double xmin,
+                             double ymin, cudaStream_t s);
+// t(x,y) = sum of shifted LUTs over the slice's atoms, then
+// e^{-Im} (cos Re, sin Re) (slice.cpp:1544-1725).  Atoms in slice order.
+cudaError_t launch_potential(double* t, const double* luts, int nx, int ny,
+                             const int32_t* atom_sx, const int32_t* atom_sy,
+                             const int32_t* atom_species, int n_atoms,
+                             cudaStream_t s);
+// Probe in k-space before the inverse transform (probe_wavefunction.cpp).
+cudaError_t launch_probe_synth(double* out, const double* kx, const double* ky,
+                               int nx, int ny, int corrected, double cs3,
+                               double cs5, double defocus, double lambda,
+                               double lambda_sq, double alpha_max_sq, double x0,
+                               double y0, cudaStream_t s);
+// out[0] = sum |a|^2 over n complex doubles (deterministic, one block).
+cudaError_t launch_norm2(const double* a, int64_t n, double* out, cudaStream_t s);
+// a *= s (n complex doubles); s read from device memory when dev_scale.
+cudaError_t launch_scale(double* a, int64_t n, double s, const double* dev_rsqrt_of,
+                         cudaStream_t st);
+cudaError_t launch_to_f32(const double* in, float* out, int64_t n_real,
+                          cudaStream_t s);
+
+// ---- detection / FEM reductions on a batch of k-space waves ----
+// For every (probe b, segment g): amp[b*ng+g] = sum |psi|, inten[...] =
+// sum |psi|^2 over pixel list idx[start[g] .. start[g+1]), FP64.
+cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t batch_stride,
+                                int nb, const int32_t* idx, const int32_t* start,
+                                int ng, double* amp, double* inten, cudaStream_t s);
+// acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
+cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
+                               int nb, int64_t npix, double* acc_a, double* acc_i,
+                               cudaStream_t s);
+
+}  // namespace msf

@@ -1,0 +1,386 @@
+"""Python binding of libmsf.so (the C ABI in include/msf.h).
+
+This is the host-side mirror of the reference's interface for the
+multislice path: ``parse_cmdline`` takes the reference's argv, ``Specimen``
+does what tem.cpp:944-1276 does (LUTs, slicing, propagators, transmission
+functions) and ``Context.run`` is ``adfstem()``.  All compute runs in the
+CUDA library; there is no CPU fallback -- if libmsf.so is missing or no GPU
+is present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmsf.so"
+CLI_PATH = HERE / "bin" / "ms-stem-fem"
+
+MSF_FP64, MSF_FP32 = 0, 1
+OUT_ADF_IMAGE = 1 << 0
+OUT_V_OMEGA, OUT_VBAR_R, OUT_V_RE = 1 << 1, 1 << 2, 1 << 3
+OUT_OMEGA_VIMAGE, OUT_V_GT17, OUT_V_RBAR = 1 << 4, 1 << 5, 1 << 6
+FEM_MODES = {"V_omega": OUT_V_OMEGA, "Vbar_r": OUT_VBAR_R, "V_re": OUT_V_RE,
+             "Omega_vimage": OUT_OMEGA_VIMAGE, "V_gt17": OUT_V_GT17,
+             "V_rbar": OUT_V_RBAR}
+_FIELD = {"V_omega": "v_omega", "Vbar_r": "vbar_r", "V_re": "v_re",
+          "Omega_vimage": "omega_vimage", "V_gt17": "v_gt17", "V_rbar": "v_rbar"}
+
+# every symbol include/msf.h declares
+EXPORTED = [
+    "msf_abi_version", "msf_last_error", "msf_status_string",
+    "msf_context_create", "msf_context_destroy", "msf_context_synchronize",
+    "msf_specimen_create", "msf_specimen_destroy", "msf_specimen_slices",
+    "msf_specimen_transmission", "msf_specimen_device_bytes", "msf_run",
+    "msf_probe", "msf_wavelength", "msf_scherzer", "msf_raster_points",
+    "msf_probe_shifts", "msf_ring_bins", "msf_parse_cmdline",
+    "msf_job_destroy", "msf_job_describe", "msf_job_output_prefix",
+    "msf_read_specimen", "msf_write_outputs", "msf_main", "msf_slice_atoms",
+    "msf_time_passes", "msf_context_transfer_bytes",
+]
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("batch", C.c_int32),
+                ("use_graphs", C.c_int32), ("hbm_budget", C.c_int64)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("voltage", C.c_double),
+                ("xperiod", C.c_double), ("yperiod", C.c_double), ("zperiod", C.c_double),
+                ("dupe_x", C.c_int32), ("dupe_y", C.c_int32), ("dupe_z", C.c_int32),
+                ("replicate_atoms", C.c_int32),
+                ("xmin", C.c_double), ("ymin", C.c_double), ("zmin", C.c_double),
+                ("min_slice", C.c_double)]
+
+
+class Atoms(C.Structure):
+    _fields_ = [("n_atoms", C.c_int64), ("q", _dp), ("z", C.POINTER(C.c_uint32))]
+
+
+class Optics(C.Structure):
+    _fields_ = [("corrected", C.c_int32), ("cs3", C.c_double), ("cs5", C.c_double),
+                ("defocus", C.c_double), ("alpha_max", C.c_double)]
+
+
+class Raster(C.Structure):
+    _fields_ = [("n_x", C.c_int32), ("n_y", C.c_int32), ("x_p", _dp), ("y_p", _dp)]
+
+
+class Detect(C.Structure):
+    _fields_ = [("outputs", C.c_uint32), ("det_inner", C.c_double),
+                ("det_outer", C.c_double), ("dr", C.c_double)]
+
+
+class Results(C.Structure):
+    _fields_ = [("adf_image", _dp), ("cap_k", C.c_int32), ("n_k", C.c_int32),
+                ("k_lower", _dp), ("bin_counts", _ip), ("v_omega", _dp), ("vbar_r", _dp),
+                ("v_re", _dp), ("omega_vimage", _dp), ("v_gt17", _dp), ("v_rbar", _dp),
+                ("final_psi", _dp), ("mean_amplitude", _dp), ("mean_intensity", _dp),
+                ("probe_slices", C.c_int64), ("kernel_launches", C.c_int64),
+                ("seconds_setup", C.c_double),
+                ("seconds_raster", C.c_double)]
+
+
+class MsfError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("msf status %d: %s" % (status, message))
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libmsf.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError("libmsf.so not built: run `make -C ms-stem-fem_b200` "
+                               "(or __graft_entry__.build())")
+        L = C.CDLL(str(LIB_PATH))
+        L.msf_last_error.restype = C.c_char_p
+        L.msf_status_string.restype = C.c_char_p
+        L.msf_context_create.argtypes = [C.POINTER(Options), C.POINTER(C.c_void_p)]
+        L.msf_context_destroy.argtypes = [C.c_void_p]
+        L.msf_context_synchronize.argtypes = [C.c_void_p]
+        L.msf_specimen_create.argtypes = [C.c_void_p, C.POINTER(Grid), C.POINTER(Atoms),
+                                          C.POINTER(C.c_void_p)]
+        L.msf_specimen_destroy.argtypes = [C.c_void_p]
+        L.msf_specimen_slices.argtypes = [C.c_void_p, _ip, _dp, _dp, _lp, C.c_int32]
+        L.msf_specimen_transmission.argtypes = [C.c_void_p, C.c_int32, _dp]
+        L.msf_specimen_device_bytes.argtypes = [C.c_void_p]
+        L.msf_specimen_device_bytes.restype = C.c_int64
+        L.msf_run.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics), C.POINTER(Raster),
+                              C.POINTER(Detect), C.POINTER(Results)]
+        L.msf_probe.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics), _dp]
+        L.msf_wavelength.argtypes = [C.c_double, _dp, _dp]
+        L.msf_wavelength.restype = None
+        L.msf_scherzer.argtypes = [C.c_int32, C.c_double, C.c_double]
+        L.msf_scherzer.restype = C.c_double
+        L.msf_raster_points.argtypes = [C.c_double, C.c_double, C.c_double, _dp, C.c_int32]
+        L.msf_probe_shifts.argtypes = [C.POINTER(Grid), C.POINTER(Raster), _lp]
+        L.msf_ring_bins.argtypes = [C.POINTER(Grid), C.c_double, _ip, _ip]
+        L.msf_parse_cmdline.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_void_p)]
+        L.msf_job_destroy.argtypes = [C.c_void_p]
+        L.msf_job_describe.argtypes = [C.c_void_p, C.POINTER(Grid), C.POINTER(Atoms),
+                                       C.POINTER(Optics), C.POINTER(Raster), C.POINTER(Detect)]
+        L.msf_job_output_prefix.argtypes = [C.c_void_p]
+        L.msf_job_output_prefix.restype = C.c_char_p
+        L.msf_read_specimen.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+        L.msf_write_outputs.argtypes = [C.c_void_p, C.POINTER(Results)]
+        L.msf_main.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(Options)]
+        L.msf_slice_atoms.argtypes = [C.c_int64, _dp, C.c_double, C.c_double, C.c_double,
+                                      _ip, _dp, _dp, _lp, _lp, C.c_int32]
+        L.msf_context_transfer_bytes.argtypes = [C.c_void_p, _lp, _lp, C.c_int32]
+        L.msf_time_passes.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise MsfError(status, lib().msf_last_error().decode(errors="replace"))
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def slice_atoms(q: np.ndarray, min_slice: float, zmin: float = 0.0, zperiod: float = 0.0):
+    """Host-only slicing (slice.cpp:469-980): boundaries, counts, atom order."""
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
+    n = q.size // 3
+    cap = max(1, n)
+    lower, thick = np.zeros(cap), np.zeros(cap)
+    counts, order = np.zeros(cap, dtype=np.int64), np.zeros(cap, dtype=np.int64)
+    ns = C.c_int32()
+    _check(lib().msf_slice_atoms(n, _p(q), zmin, zperiod, min_slice, C.byref(ns), _p(lower),
+                                 _p(thick), counts.ctypes.data_as(_lp),
+                                 order.ctypes.data_as(_lp), cap))
+    k = ns.value
+    return {"n": k, "lower": lower[:k], "thickness": thick[:k], "counts": counts[:k],
+            "order": order[:n]}
+
+
+def wavelength(voltage: float):
+    lam, gam = C.c_double(), C.c_double()
+    lib().msf_wavelength(voltage, C.byref(lam), C.byref(gam))
+    return lam.value, gam.value
+
+
+class Job:
+    """A parsed reference command line plus its specimen (tem.cpp:81-1378)."""
+
+    def __init__(self, argv):
+        argv = [str(a) for a in argv]
+        if not argv or not argv[0].endswith("ms-stem-fem"):
+            argv = ["ms-stem-fem"] + argv
+        arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+        h = C.c_void_p()
+        _check(lib().msf_parse_cmdline(len(argv), arr, C.byref(h)))
+        self._h = h
+        self.grid, self.atoms = Grid(), Atoms()
+        self.optics, self.raster, self.detect = Optics(), Raster(), Detect()
+        _check(lib().msf_job_describe(h, C.byref(self.grid), C.byref(self.atoms),
+                                      C.byref(self.optics), C.byref(self.raster),
+                                      C.byref(self.detect)))
+        self.prefix = lib().msf_job_output_prefix(h).decode()
+
+    @property
+    def n_probes(self):
+        return self.raster.n_x * self.raster.n_y
+
+    def positions(self):
+        n = self.atoms.n_atoms
+        q = np.ctypeslib.as_array(self.atoms.q, shape=(3 * n,)).copy().reshape(n, 3)
+        z = np.ctypeslib.as_array(self.atoms.z, shape=(n,)).copy()
+        return q, z
+
+    def raster_points(self):
+        r = self.raster
+        return (np.ctypeslib.as_array(r.x_p, shape=(r.n_x,)).copy(),
+                np.ctypeslib.as_array(r.y_p, shape=(r.n_y,)).copy())
+
+    def fem_modes(self):
+        return [m for m, b in FEM_MODES.items() if self.detect.outputs & b]
+
+    def oracle_job(self) -> dict:
+        """The same job as a plain dict (the CPU oracle's input format)."""
+        xp, yp = self.raster_points()
+        g, o, d = self.grid, self.optics, self.detect
+        return dict(nx=g.nx, ny=g.ny, voltage=g.voltage, xperiod=g.xperiod,
+                    yperiod=g.yperiod, xperiod_duped=g.xperiod * max(1, g.dupe_x),
+                    yperiod_duped=g.yperiod * max(1, g.dupe_y), xmin=g.xmin, ymin=g.ymin,
+                    min_slice=g.min_slice, corrected=o.corrected, cs3=o.cs3, cs5=o.cs5,
+                    defocus=o.defocus, alpha_max=o.alpha_max, det_inner=d.det_inner,
+                    det_outer=d.det_outer, dr=d.dr, x_p=xp, y_p=yp,
+                    images=bool(d.outputs & OUT_ADF_IMAGE), fem_modes=self.fem_modes())
+
+    def write_outputs(self, res: "RunResult"):
+        _check(lib().msf_write_outputs(self._h, C.byref(res._struct)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.msf_job_destroy(h)
+            self._h = None
+
+
+class Context:
+    """One CUDA device, one stream, one wavefield precision."""
+
+    def __init__(self, device=0, precision="fp64", batch=0, graphs=True, hbm_budget=0):
+        opt = Options(device, MSF_FP32 if precision == "fp32" else MSF_FP64, batch,
+                      1 if graphs else 0, hbm_budget)
+        h = C.c_void_p()
+        _check(lib().msf_context_create(C.byref(opt), C.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().msf_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def transfer_bytes(self, reset=False):
+        """(host->device, device->host) bytes copied since the last reset."""
+        h, d = C.c_int64(), C.c_int64()
+        _check(lib().msf_context_transfer_bytes(self._h, C.byref(h), C.byref(d), int(reset)))
+        return h.value, d.value
+
+    def synchronize(self):
+        _check(lib().msf_context_synchronize(self._h))
+
+    def specimen(self, grid: Grid, q: np.ndarray, z: np.ndarray) -> "Specimen":
+        return Specimen(self, grid, q, z)
+
+    def run(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
+            want_final_psi=False, want_means=False, cap_k=8192) -> "RunResult":
+        nx, ny = spec.grid.nx, spec.grid.ny
+        n_r = raster.n_x * raster.n_y
+        out = RunResult(n_r, cap_k, nx, ny, want_final_psi, want_means)
+        _check(lib().msf_run(self._h, spec._h, C.byref(optics), C.byref(raster),
+                             C.byref(detect), C.byref(out._struct)))
+        out.finish(raster, detect)
+        return out
+
+    def time_passes(self, spec: "Specimen", nb: int, reps: int = 10):
+        """Mean ms per launch of the fused row and column slice passes."""
+        r, c = C.c_double(), C.c_double()
+        _check(lib().msf_time_passes(self._h, spec._h, nb, reps, C.byref(r), C.byref(c)))
+        return r.value, c.value
+
+    def probe(self, spec: "Specimen", optics: Optics) -> np.ndarray:
+        out = np.zeros(2 * spec.grid.nx * spec.grid.ny)
+        _check(lib().msf_probe(self._h, spec._h, C.byref(optics), _p(out)))
+        return out.reshape(spec.grid.nx, spec.grid.ny, 2)
+
+
+class Specimen:
+    """Device-resident LUTs, slices, propagators and transmission functions."""
+
+    def __init__(self, ctx: Context, grid: Grid, q: np.ndarray, z: np.ndarray):
+        self.ctx = ctx
+        self.grid = grid
+        self._q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
+        self._z = np.ascontiguousarray(z, dtype=np.uint32)
+        atoms = Atoms(len(self._z), _p(self._q), self._z.ctypes.data_as(C.POINTER(C.c_uint32)))
+        h = C.c_void_p()
+        _check(lib().msf_specimen_create(ctx._h, C.byref(grid), C.byref(atoms), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().msf_specimen_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def slices(self):
+        n = C.c_int32()
+        lib().msf_specimen_slices(self._h, C.byref(n), None, None, None, 0)
+        k = n.value
+        lower, thick = np.zeros(k), np.zeros(k)
+        counts = np.zeros(k, dtype=np.int64)
+        _check(lib().msf_specimen_slices(self._h, C.byref(n), _p(lower), _p(thick),
+                                         counts.ctypes.data_as(_lp), k))
+        return {"n": k, "lower": lower, "thickness": thick, "counts": counts}
+
+    def transmission(self, s: int) -> np.ndarray:
+        out = np.zeros(2 * self.grid.nx * self.grid.ny)
+        _check(lib().msf_specimen_transmission(self._h, s, _p(out)))
+        return out.reshape(self.grid.nx, self.grid.ny, 2)
+
+    def device_bytes(self) -> int:
+        return lib().msf_specimen_device_bytes(self._h)
+
+
+class RunResult:
+    def __init__(self, n_r, cap_k, nx, ny, want_psi, want_means):
+        self.adf_image = np.zeros(n_r)
+        self.k_lower = np.zeros(cap_k)
+        self.bin_counts = np.zeros(cap_k, dtype=np.int32)
+        self._v = {m: np.full(cap_k, np.nan) for m in FEM_MODES}
+        self.final_psi = np.zeros(2 * nx * ny) if want_psi else None
+        self.mean_amplitude = np.zeros(nx * ny) if want_means else None
+        self.mean_intensity = np.zeros(nx * ny) if want_means else None
+        s = Results()
+        s.adf_image = _p(self.adf_image)
+        s.cap_k = cap_k
+        s.k_lower = _p(self.k_lower)
+        s.bin_counts = self.bin_counts.ctypes.data_as(_ip)
+        for m, f in _FIELD.items():
+            setattr(s, f, _p(self._v[m]))
+        if want_psi:
+            s.final_psi = _p(self.final_psi)
+        if want_means:
+            s.mean_amplitude = _p(self.mean_amplitude)
+            s.mean_intensity = _p(self.mean_intensity)
+        self._struct = s
+        self._shape = (nx, ny)
+
+    def finish(self, raster, detect):
+        s = self._struct
+        self.n_k = s.n_k
+        self.probe_slices = s.probe_slices
+        self.kernel_launches = s.kernel_launches
+        self.seconds_raster = s.seconds_raster
+        self.adf_image_2d = self.adf_image.reshape(raster.n_x, raster.n_y)
+        self.v = {m: self._v[m][:self.n_k] for m in FEM_MODES if detect.outputs & FEM_MODES[m]}
+        self.k = self.k_lower[:self.n_k]
+        self.counts = self.bin_counts[:self.n_k]
+        if self.final_psi is not None:
+            self.final_psi_2d = self.final_psi.reshape(*self._shape, 2)
+
+
+def run_job(argv, precision="fp64", device=0, batch=0, graphs=True, write=False,
+            want_final_psi=False):
+    """Parse a reference command line and run it end to end on the GPU."""
+    job = Job(argv)
+    ctx = Context(device=device, precision=precision, batch=batch, graphs=graphs)
+    q, z = job.positions()
+    spec = ctx.specimen(job.grid, q, z)
+    res = ctx.run(spec, job.optics, job.raster, job.detect, want_final_psi=want_final_psi)
+    if write:
+        job.write_outputs(res)
+    return job, spec, res, ctx
+
+
+def main(argv, precision="fp64", device=0, batch=0) -> int:
+    """The whole drop-in program (msf_main); returns the exit status."""
+    argv = [str(a) for a in argv]
+    arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+    opt = Options(device, MSF_FP32 if precision == "fp32" else MSF_FP64, batch, 1, 0)
+    return lib().msf_main(len(argv), arr, C.byref(opt))

@@ -1,0 +1,150 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures in tests/golden/ by running the reference's
+own sources (built by oracle/Makefile into oracle/_ref/ms-stem-fem-ref) on
+seeded specimens.
+
+    make -C oracle && python tests/golden/make_golden.py [case ...]
+
+Each case writes ``<case>.npz`` (outputs of the reference run: raw FP64 ADF
+image, every FEM V(k) text file, slice boundaries, optionally one slice's
+transmission function) and ``<case>.json`` (argv, specimen recipe, sha256 of
+the specimen file).  Small specimens are committed as ``<case>.data``; large
+ones are regenerated from their seed by the tests and checked against the
+recorded sha256.  Needs the reference sources; the GPU box only reads the
+committed fixtures.
+"""
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT / "ms-stem-fem_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+import specimen  # noqa: E402
+import oracle  # noqa: E402
+
+FEM_ALL = ["--V_omega", "--Vbar_r", "--V_re", "--Omega_vimage", "--V_gt17", "--V_rbar"]
+
+# name -> (specimen recipe, argv after "-a <file> --output_prefix <name>",
+#          commit the specimen file?, dump transmission of this slice or None)
+CASES = {
+    # configuration 1: plain ADF-STEM, 780 Si in 25 A, 256^2, 16x16 probes
+    "c1": (dict(n=780, box=(25, 25, 25), seed=1),
+           "-m 256 256 200000 --adfstemuncorr --cs3 1.3e7 --scherzer_defocus "
+           "--alphamax 0.010 --rasterspacing 1.5625 --minslice 2.0 --images", True, None),
+    # every FEM mode on a small grid; alpha_max zeroes the first bins
+    "fem128": (dict(n=780, box=(25, 25, 25), seed=1),
+               "-m 128 128 200000 --adfstemuncorrfem " + " ".join(FEM_ALL) +
+               " --cs3 1.3e7 --scherzer_defocus --alphamax 0.010 --rasterspacing 6.25 "
+               "--minslice 2.0 --images", True, 2),
+    # aberration-corrected probe with Scherzer Cs3/defocus/aperture
+    "corr": (dict(n=780, box=(25, 25, 25), seed=1),
+             "-m 128 128 200000 --adfstemcorrfem --V_omega --V_re --cs5 5e7 --scherzer_cs3 "
+             "--scherzer_defocus --scherzer_alphamax --rasterspacing 6.25 --minslice 2.0 "
+             "--images", True, None),
+    # non-square grid (sqrt(NxNy) scaling, different k steps along x and y)
+    "rect": (dict(n=780, box=(25, 25, 25), seed=1),
+             "-m 128 64 200000 --adfstemuncorrfem --V_omega --Vbar_r --cs3 1.3e7 --defocus 300 "
+             "--alphamax 0.012 --rasterspacing 5 --minslice 2.0 --images --dr 1.0", True, None),
+    # two species (Si + O) and 300 kV
+    "sio": (dict(n=400, box=(20, 20, 20), seed=7, two_species=True),
+            "-m 128 128 300000 --adfstemuncorrfem --V_omega --V_gt17 --cs3 1.3e7 "
+            "--scherzer_defocus --scherzer_alphamax --rasterspacing 5 --minslice 2.0 --images",
+            True, 0),
+    # --dupe 2 1 1 in an FEM run replicates the atoms; raster uses one cell
+    "dupe": (dict(n=390, box=(25, 25, 12.5), seed=11),
+             "-m 128 64 200000 --adfstemuncorrfem --V_omega --dupe 2 1 1 --cs3 1.3e7 "
+             "--scherzer_defocus --alphamax 0.010 --rasterspacing 6.25 --minslice 2.0 --images",
+             True, None),
+    # configuration 2's specimen and grid on a 2x2 raster (the full 64x64
+    # raster would take hours on one CPU core)
+    "c2_small": (dict(n=50000, box=(100, 100, 100), seed=2),
+                 "-m 1024 1024 200000 --adfstemuncorrfem --V_omega --V_re --cs3 1.3e7 "
+                 "--defocus 0 --alphamax 0.0015 --rasterspacing 50 --minslice 2.0 --dr 1.2065",
+                 False, None),
+}
+
+
+def make_specimen_file(recipe, path):
+    pos = specimen.make_specimen(path, recipe["n"], recipe["box"], seed=recipe["seed"])
+    if recipe.get("two_species"):
+        # every third atom becomes oxygen (mass 15.999 -> Z = 8)
+        text = Path(path).read_text().splitlines()
+        out, in_atoms, k = [], False, 0
+        for line in text:
+            if line.strip() == "1 atom types":
+                line = "2 atom types"
+            if line.strip() == "1 28.0855":
+                line = "1 28.0855\n2 15.999"
+            if in_atoms and line.strip():
+                parts = line.split()
+                if k % 3 == 2:
+                    parts[1] = "2"
+                line = " ".join(parts)
+                k += 1
+            if line.strip() == "Atoms":
+                in_atoms = True
+            out.append(line)
+        Path(path).write_text("\n".join(out) + "\n")
+    return pos
+
+
+def sha256(path):
+    return hashlib.sha256(Path(path).read_bytes()).hexdigest()
+
+
+def run_case(name):
+    recipe, args, commit, tslice = CASES[name]
+    work = Path(tempfile.mkdtemp(prefix="golden_" + name))
+    spec = work / (name + ".data")
+    make_specimen_file(recipe, spec)
+    argv = ["-a", spec.name, "--output_prefix", name] + args.split()
+    env = {"MSF_REF_DUMP_SLICES": str(work / "slices.txt")}
+    if tslice is not None:
+        env["MSF_REF_DUMP_T"] = str(work / "t_")
+    r = oracle.run_reference(argv, cwd=work, env_extra=env)
+    if r["returncode"] != 0:
+        raise RuntimeError("reference failed for %s:\n%s\n%s" % (name, r["stdout"], r["stderr"]))
+    out = {}
+    corr = any(a in ("--adfstemcorr", "--adfstemcorrfem") for a in args.split())
+    prefix = work / (name + ("_adfstem_corr" if corr else "_adfstem_uncorr"))
+    for f in work.iterdir():
+        if f.name.endswith("_stem_image_output.f64"):
+            out["adf_image"] = np.fromfile(f)
+            prefix = Path(str(f)[: -len("_stem_image_output.f64")])
+    for f in sorted(work.glob("*_fem_*.txt")):
+        mode = f.stem.split("_fem_")[1]
+        out[mode] = oracle.read_variance_txt(f)
+    sl = np.loadtxt(work / "slices.txt", ndmin=2)
+    out["slice_lower"], out["slice_thickness"], out["slice_count"] = sl[:, 0], sl[:, 1], sl[:, 2]
+    if tslice is not None:
+        t = np.fromfile(work / ("t_%d.c128" % (tslice + 1)))
+        out["transmission_slice"] = np.array(tslice)
+        out["transmission"] = t
+    np.savez_compressed(HERE / (name + ".npz"), **out)
+    meta = dict(case=name, argv=argv, recipe=recipe, specimen_sha256=sha256(spec),
+                committed_specimen=commit, prefix=prefix.name,
+                adfstem_seconds=r["adfstem_seconds"], probes=r["probes"], slices=r["slices"])
+    (HERE / (name + ".json")).write_text(json.dumps(meta, indent=1) + "\n")
+    if commit:
+        shutil.copy(spec, HERE / (name + ".data"))
+    shutil.rmtree(work)
+    print(name, "ok", r["adfstem_seconds"], "s", sorted(out))
+
+
+def main():
+    names = sys.argv[1:] or list(CASES)
+    for n in names:
+        run_case(n)
+
+
+if __name__ == "__main__":
+    main()

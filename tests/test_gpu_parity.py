@@ -1,0 +1,140 @@
+"""CUDA path against the reference's own results (golden fixtures) and the
+CPU oracle.  Tolerances: ADF image and V(k) within
+1e-5 relative on the FP64 path and 1e-4 on the FP32 path; slicing, pixel
+snaps and bins bit-exact.  V(k) also gets an absolute floor for bins where
+V itself is at the cancellation floor of n*sum(A^2)/sum(A)^2 - 1."""
+import subprocess
+
+import numpy as np
+import pytest
+
+import msf
+import oracle
+from conftest import (ROOT, assert_variance_close, case_dir, golden_cases, load_case,
+                      rel_err)
+
+pytestmark = pytest.mark.gpu
+
+TOL = {
+    "fp64": dict(adf=1e-5, v_rtol=1e-5, v_atol=1e-12),
+    "fp32": dict(adf=1e-4, v_rtol=1e-4, v_atol=1e-7),
+}
+MODES = ["V_omega", "Vbar_r", "V_re", "Omega_vimage", "V_gt17", "V_rbar"]
+
+
+def run_case(name, golden_tmp, precision, batch=0, graphs=True, want_psi=False):
+    meta, ref = load_case(name)
+    d = case_dir(name, golden_tmp)
+    argv = [a if a != meta["argv"][1] else str(d / a) for a in meta["argv"]]
+    job, spec, res, ctx = msf.run_job(argv, precision=precision, batch=batch, graphs=graphs,
+                                      want_final_psi=want_psi)
+    return meta, ref, job, spec, res, ctx
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", golden_cases())
+def test_matches_reference(name, precision, golden_tmp):
+    meta, ref, job, spec, res, ctx = run_case(name, golden_tmp, precision)
+    tol = TOL[precision]
+    sl = spec.slices()
+    assert np.array_equal(sl["lower"], ref["slice_lower"])
+    assert np.array_equal(sl["thickness"], ref["slice_thickness"])
+    assert np.array_equal(sl["counts"], ref["slice_count"].astype(np.int64))
+    if "adf_image" in ref:
+        err = rel_err(res.adf_image, ref["adf_image"]).max()
+        print("%s %s ADF max rel err %.3e" % (name, precision, err))
+        assert err <= tol["adf"]
+    for mode in MODES:
+        if mode in ref:
+            np.testing.assert_allclose(res.k, ref[mode][:, 0], rtol=1e-10, atol=0)
+            got, want = res.v[mode], ref[mode][:, 1]
+            m = ~np.isnan(want) & (want != 0)
+            if m.any():
+                print("%s %s %s max rel err %.3e" % (name, precision, mode,
+                                                     rel_err(got[m], want[m]).max()))
+            assert_variance_close(got, want, tol["v_rtol"], tol["v_atol"],
+                                  what="%s %s %s" % (name, precision, mode))
+    if "transmission" in ref and precision == "fp64":
+        t = spec.transmission(int(ref["transmission_slice"])).ravel()
+        assert np.abs(t - ref["transmission"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_exit_wave_matches_oracle(precision, golden_tmp):
+    meta, ref, job, spec, res, ctx = run_case("rect", golden_tmp, precision, want_psi=True)
+    ojob, q, z = oracle.job_from_argv(meta["argv"], case_dir("rect", golden_tmp))
+    out = oracle.run(ojob, q, z, want_last_psi=True)
+    a = res.final_psi_2d[..., 0] + 1j * res.final_psi_2d[..., 1]
+    b = out["last_psi"][..., 0] + 1j * out["last_psi"][..., 1]
+    err = np.abs(a - b).max() / np.abs(b).max()
+    print("exit wave %s max err / max |psi| = %.3e" % (precision, err))
+    assert err <= (1e-10 if precision == "fp64" else 2e-5)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_probe_matches_oracle(precision, golden_tmp):
+    meta, ref, job, spec, res, ctx = run_case("corr", golden_tmp, precision)
+    p = ctx.probe(spec, job.optics)
+    ojob, q, z = oracle.job_from_argv(meta["argv"], case_dir("corr", golden_tmp))
+    o = oracle.probe(ojob)
+    assert np.abs(p - o).max() <= 1e-12 * np.abs(o).max()
+
+
+def test_batching_and_graphs_do_not_change_results(golden_tmp):
+    """A probe's result is the same alone and in any batch, with or without
+    the captured graph."""
+    base = run_case("fem128", golden_tmp, "fp32", batch=16, graphs=False)[4]
+    for batch, graphs in [(1, False), (3, True), (5, True), (16, True)]:
+        r = run_case("fem128", golden_tmp, "fp32", batch=batch, graphs=graphs)[4]
+        assert np.array_equal(r.adf_image, base.adf_image), (batch, graphs)
+        for m in ("V_omega", "Vbar_r"):
+            assert np.array_equal(r.v[m], base.v[m], equal_nan=True), (batch, graphs, m)
+        for m in ("V_re", "Omega_vimage", "V_gt17", "V_rbar"):
+            np.testing.assert_allclose(r.v[m], base.v[m], rtol=1e-12, equal_nan=True)
+
+
+def test_cli_writes_reference_outputs(golden_tmp, tmp_path):
+    meta, ref = load_case("fem128")
+    d = case_dir("fem128", golden_tmp)
+    cli = ROOT / "ms-stem-fem_b200" / "bin" / "ms-stem-fem"
+    p = subprocess.run([str(cli)] + meta["argv"], cwd=d, capture_output=True, text=True)
+    assert p.returncode == 0, p.stdout + p.stderr
+    for mode in MODES:
+        t = oracle.read_variance_txt(d / (meta["prefix"] + "_fem_%s.txt" % mode))
+        assert_variance_close(t[:, 1], ref[mode][:, 1], 1e-5, 1e-12, what=mode)
+    img = np.fromfile(d / (meta["prefix"] + "_stem_image_output.f64"))
+    assert rel_err(img, ref["adf_image"]).max() <= 1e-5
+    # the TIFF holds the reference's 16-bit min/max quantisation, rows bottom-up
+    tif = (d / (meta["prefix"] + "_stem_image_output.tif")).read_bytes()
+    assert tif[:4] == b"II*\x00"
+    n = int(round(np.sqrt(img.size)))
+    want = np.floor((ref["adf_image"] - ref["adf_image"].min()) *
+                    (65535.0 / (ref["adf_image"].max() - ref["adf_image"].min())) + 0.5)
+    want = want.reshape(n, n)[::-1].ravel()
+    got = np.frombuffer(tif[8:8 + 2 * img.size], dtype="<u2").astype(float)
+    assert np.abs(got - want).max() <= 1
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [1024, 2048])
+def test_vacuum_propagation_preserves_norm(n, precision):
+    """Size-independent property at full size: with no atoms the exit wave's
+    k-space norm is the probe's, 1 (the aperture lies inside the band limit),
+    and the dark-field signal vanishes."""
+    ctx = msf.Context(precision=precision, batch=4)
+    L = n * 0.09765625
+    g = msf.Grid(nx=n, ny=n, voltage=200000.0, xperiod=L, yperiod=L, zperiod=100.0,
+                 dupe_x=1, dupe_y=1, dupe_z=1, replicate_atoms=0, min_slice=2.0)
+    spec = ctx.specimen(g, np.zeros((0, 3)), np.zeros(0, dtype=np.uint32))
+    assert spec.slices()["n"] == 1
+    lam, _ = msf.wavelength(200000.0)
+    o = msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0, defocus=0.87 * np.sqrt(1.3e7 * lam),
+                   alpha_max=0.010)
+    xp = np.array([0.0, L / 3, L / 2])
+    r = msf.Raster(3, 3, xp.ctypes.data_as(msf._dp), xp.ctypes.data_as(msf._dp))
+    det = msf.Detect(outputs=msf.OUT_ADF_IMAGE, det_inner=0.04, det_outer=0.2, dr=0.7071)
+    res = ctx.run(spec, o, r, det, want_final_psi=True)
+    psi = res.final_psi_2d
+    norm = (psi ** 2).sum()
+    assert abs(norm - 1.0) <= (1e-12 if precision == "fp64" else 1e-5)
+    assert res.adf_image.max() <= (1e-20 if precision == "fp64" else 1e-9)
