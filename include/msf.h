@@ -124,6 +124,9 @@ typedef struct {
   double* final_psi;       /* 2*nx*ny: last probe's exit wave in k-space      */
   double* mean_amplitude;  /* nx*ny: raster mean of |psi(k)| (FEM pixel modes)*/
   double* mean_intensity;  /* nx*ny: raster mean of |psi(k)|^2                */
+  double* ring_amplitude;  /* n_x*n_y*cap_k: per probe, sum |psi| per ring,
+                              before the aperture zeroing (FEM runs)         */
+  double* ring_intensity;  /* n_x*n_y*cap_k: per probe, sum |psi|^2 per ring  */
   int64_t probe_slices;    /* out: probe*slice propagations performed          */
   int64_t kernel_launches; /* out: CUDA kernels this call launched (incl. the
                               kernels inside replayed graphs)                 */

@@ -164,7 +164,11 @@ msf_status msf_specimen_transmission(const msf_specimen* spec, int32_t slice, do
     std::vector<float> tmp(2 * plane);
     e = cudaMemcpy(tmp.data(), spec->t.as<float>() + 2 * plane * slice, 8 * plane,
                    cudaMemcpyDeviceToHost);
-    for (int64_t k = 0; k < 2 * plane; ++k) out[k] = tmp[k];
+    // FP32 contexts store tau = t - 1 (split-wave passes)
+    for (int64_t k = 0; k < plane; ++k) {
+      out[2 * k] = (double)tmp[2 * k] + 1.0;
+      out[2 * k + 1] = tmp[2 * k + 1];
+    }
   }
   if (e != cudaSuccess) {
     set_error(std::string("cudaMemcpy: ") + cudaGetErrorString(e));

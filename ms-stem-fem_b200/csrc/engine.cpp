@@ -277,7 +277,8 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
     MSF_CUDA(launch_row(true, ROW_INV, a, ctx->stream));
     a.scale = 1.0;
     if (!ctx->fp64)
-      MSF_CUDA(launch_to_f32(t64, spec->t.as<float>() + 2 * plane * s, 2 * plane, ctx->stream));
+      MSF_CUDA(launch_to_f32_minus_one(t64, spec->t.as<float>() + 2 * plane * s, plane,
+                                       ctx->stream));
   }
 
   // propagators (slice.cpp:1293-1363)
@@ -337,6 +338,14 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   DevBuf psi;
   MSF_TRY(ctx->alloc(&psi, cbytes * plane * nb));
   MSF_CUDA(cudaMemsetAsync(psi.p, 0, psi.bytes, ctx->stream));
+  DevBuf psi0, zshift;
+  if (!fp64) {  // split-wave row pass reads one vacuum plane and the shifts
+    MSF_TRY(ctx->alloc(&psi0, 8 * plane));
+    MSF_TRY(ctx->alloc(&zshift, sizeof(int32_t) * 2 * nb));
+    MSF_CUDA(cudaMemsetAsync(psi0.p, 0, psi0.bytes, ctx->stream));
+    MSF_CUDA(cudaMemsetAsync(zshift.p, 0, zshift.bytes, ctx->stream));
+  }
+  const RowOp rop = fp64 ? ROW_SLICE : ROW_SPLIT;
   PassArgs row, col;
   row.psi = col.psi = psi.p;
   row.batch_stride = col.batch_stride = plane;
@@ -347,6 +356,8 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
   row.inv_s = col.inv_s = 1.0 / g.s;
   row.trans = spec->t.p;
+  row.psi0 = psi0.p;
+  row.shifts = zshift.as<int32_t>();
   col.mask_lo = spec->mask_lo.as<int32_t>();
   col.mask_hi = spec->mask_hi.as<int32_t>();
   col.px = spec->prop.p;
@@ -354,12 +365,12 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   std::vector<cudaEvent_t> ev(2 * reps + 2);
   for (auto& e : ev) MSF_CUDA(cudaEventCreate(&e));
   // warm-up
-  MSF_CUDA(launch_row(fp64, ROW_SLICE, row, ctx->stream));
+  MSF_CUDA(launch_row(fp64, rop, row, ctx->stream));
   MSF_CUDA(launch_col(fp64, COL_SLICE, col, ctx->stream));
   double tr = 0, tc = 0;
   for (int r = 0; r < reps; ++r) {
     MSF_CUDA(cudaEventRecord(ev[2 * r], ctx->stream));
-    MSF_CUDA(launch_row(fp64, ROW_SLICE, row, ctx->stream));
+    MSF_CUDA(launch_row(fp64, rop, row, ctx->stream));
     MSF_CUDA(cudaEventRecord(ev[2 * r + 1], ctx->stream));
     MSF_CUDA(launch_col(fp64, COL_SLICE, col, ctx->stream));
     MSF_CUDA(cudaEventRecord(ev[2 * r + 2], ctx->stream));
@@ -397,13 +408,54 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   MSF_CUDA(cudaSetDevice(ctx->device));
 
   // probe
-  DevBuf probe64, probe32;
+  DevBuf probe64;
   MSF_TRY(build_probe(ctx, spec, optics, &probe64));
   const void* probe = probe64.p;
+  int64_t setup_launches = 5;
+
+  // FP32 runs carry only the scattered part of each wave; the vacuum part
+  // psi0 (the probe propagated with t = 1) is the same for every probe up to
+  // its integer shift, so it is built once here in FP64: psi0_tab[s] is the
+  // real-space vacuum wave entering slice s (in the scale of the inverse-
+  // transformed buffer) and psi0k the vacuum exit wave in k-space.
+  DevBuf psi0_tab, psi0k, prop64;
   if (!fp64) {
-    MSF_TRY(ctx->alloc(&probe32, 8 * plane));
-    MSF_CUDA(launch_to_f32(probe64.as<double>(), probe32.as<float>(), 2 * plane, ctx->stream));
-    probe = probe32.p;
+    MSF_TRY(ctx->alloc(&psi0_tab, 8 * plane * (size_t)S));
+    MSF_TRY(ctx->alloc(&psi0k, 16 * plane));
+    MSF_TRY(upload(ctx, &prop64, spec->hprop));
+    MSF_CUDA(cudaMemcpyAsync(psi0k.p, probe64.p, 16 * plane, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+    MSF_CUDA(launch_scale(psi0k.as<double>(), plane, g.nxny / g.s, nullptr, ctx->stream));
+    PassArgs v;
+    v.psi = psi0k.p;
+    v.batch_stride = plane;
+    v.nb = 1;
+    v.nx = g.nx;
+    v.ny = g.ny;
+    v.mask_lo = spec->mask_lo.as<int32_t>();
+    v.mask_hi = spec->mask_hi.as<int32_t>();
+    v.inv_s = 1.0 / (g.s * g.s);  // Q(1, psi) = psi/s, then FFT2 and /s
+    const void *tw_y = nullptr, *tw_x = nullptr;
+    MSF_TRY(ctx->twiddles(g.ny, true, &tw_y));
+    MSF_TRY(ctx->twiddles(g.nx, true, &tw_x));
+    setup_launches += 1;
+    for (int s = 0; s < S; ++s) {
+      MSF_CUDA(launch_to_f32(psi0k.as<double>(), psi0_tab.as<float>() + 2 * plane * s,
+                             2 * plane, ctx->stream));
+      v.tw = tw_y;
+      MSF_CUDA(launch_row(true, ROW_FWD, v, ctx->stream));
+      v.tw = tw_x;
+      v.px = prop64.as<double>() + 2 * (size_t)(g.nx + g.ny) * s;
+      v.py = prop64.as<double>() + 2 * (size_t)(g.nx + g.ny) * s + 2 * g.nx;
+      MSF_CUDA(launch_col(true, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, v, ctx->stream));
+      setup_launches += 3;
+      if (s + 1 < S) {
+        v.tw = tw_y;
+        v.scale = 1.0;
+        MSF_CUDA(launch_row(true, ROW_INV, v, ctx->stream));
+        setup_launches += 1;
+      }
+    }
   }
 
   // per-probe pixel shifts
@@ -476,17 +528,31 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     row.shifts = shifts_dev;
     for (int s = 0; s < S; ++s) {
       row.trans = tbase + cbytes * plane * s;
-      MSF_CUDA(launch_row(fp64, s == 0 ? ROW_SLICE_FIRST : ROW_SLICE, row, ctx->stream));
+      RowOp op;
+      if (fp64) {
+        op = s == 0 ? ROW_SLICE_FIRST : ROW_SLICE;
+      } else {
+        op = s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT;
+        row.psi0 = psi0_tab.as<float>() + 2 * plane * s;
+      }
+      MSF_CUDA(launch_row(fp64, op, row, ctx->stream));
       col.px = pbase + prop_stride * s;
       col.py = pbase + prop_stride * s + cbytes * g.nx;
       MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
     }
+    SplitK sk;
+    if (!fp64) {
+      sk.psi0k = psi0k.as<double>();
+      sk.shifts = shifts_dev;
+      sk.nx = g.nx;
+      sk.ny = g.ny;
+    }
     MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, d_seg_idx.as<int32_t>(),
-                                 d_seg_start.as<int32_t>(), n_seg, amp_out, int_out,
+                                 d_seg_start.as<int32_t>(), n_seg, amp_out, int_out, sk,
                                  ctx->stream));
     if (pix_modes)
       MSF_CUDA(launch_pixel_accum(fp64, psi.p, plane, nb, plane, d_acc_a.as<double>(),
-                                  d_acc_i.as<double>(), ctx->stream));
+                                  d_acc_i.as<double>(), sk, ctx->stream));
     return MSF_OK;
   };
   if (S <= 0) { set_error("specimen has no slices"); return MSF_ERR_ARG; }
@@ -551,16 +617,22 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     MSF_CUDA(cudaMemcpyAsync(acc_i.data(), d_acc_i.p, plane * sizeof(double),
                              cudaMemcpyDeviceToHost, ctx->stream));
   }
-  std::vector<float> last32;
   if (res->final_psi) {
     const int last = (int)((n_probes - 1) % B);
     if (fp64) {
       MSF_CUDA(cudaMemcpyAsync(res->final_psi, psi.as<double>() + 2 * plane * last,
                                16 * plane, cudaMemcpyDeviceToHost, ctx->stream));
     } else {
-      last32.resize(2 * plane);
-      MSF_CUDA(cudaMemcpyAsync(last32.data(), psi.as<float>() + 2 * plane * last, 8 * plane,
-                               cudaMemcpyDeviceToHost, ctx->stream));
+      // exit wave = scattered part + the vacuum part at this probe's shift
+      DevBuf full;
+      MSF_TRY(ctx->alloc(&full, 16 * plane));
+      const int64_t pl = n_probes - 1;
+      MSF_CUDA(launch_assemble_split(psi.as<float>() + 2 * plane * last, psi0k.as<double>(),
+                                     g.nx, g.ny, shifts[2 * pl], shifts[2 * pl + 1],
+                                     full.as<double>(), ctx->stream));
+      MSF_CUDA(cudaMemcpyAsync(res->final_psi, full.p, 16 * plane, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+      MSF_CUDA(cudaStreamSynchronize(ctx->stream));
     }
   }
   MSF_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -568,8 +640,6 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   MSF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  if (!last32.empty())
-    for (int64_t k = 0; k < 2 * plane; ++k) res->final_psi[k] = last32[k];
   res->seconds_raster = 1e-3 * ms;
   res->seconds_setup = 0;
   res->probe_slices = n_probes * S;
@@ -577,7 +647,7 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     const int64_t n_batches = (n_probes + B - 1) / B;
     // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:
     // 2*S slice passes, the segment sums and (pixel modes) the accumulation
-    res->kernel_launches = 5 + (fp64 ? 0 : 1) + n_batches * (2 * S + 1 + (pix_modes ? 1 : 0));
+    res->kernel_launches = setup_launches + n_batches * (2 * S + 1 + (pix_modes ? 1 : 0));
     ctx->d2h_bytes += (int64_t)(8 + 2 * amp.size() * sizeof(double)) +
                       (pix_modes ? 16 * plane : 0) +
                       (res->final_psi ? (int64_t)cbytes * plane : 0);
@@ -601,6 +671,11 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     if (res->k_lower) res->k_lower[k] = rings.bounds[k];
     if (res->bin_counts) res->bin_counts[k] = cnt[k];
   }
+  for (int64_t p = 0; p < n_probes; ++p)
+    for (int k = 0; k < n_k; ++k) {
+      if (res->ring_amplitude) res->ring_amplitude[p * res->cap_k + k] = amp[p * n_seg + k];
+      if (res->ring_intensity) res->ring_intensity[p * res->cap_k + k] = inten[p * n_seg + k];
+    }
   const double n_r = (double)(size_t)n_probes;
   if (det->outputs & (MSF_OUT_V_OMEGA | MSF_OUT_VBAR_R)) {
     std::vector<double> sa2(n_k, 0.0), sa(n_k, 0.0), vs(n_k, 0.0);

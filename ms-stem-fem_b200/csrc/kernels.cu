@@ -78,11 +78,41 @@ row_kernel(const PassArgs a) {
       const int iy = (y < sy) ? y + N - sy : y - sy;
       v[m] = cscale(__ldg(prow + iy), fs);
     }
+  } else if constexpr (OP == ROW_SPLIT_FIRST) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
   } else {
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = row[t + T * m];
   }
-  if constexpr (OP == ROW_FWD) {
+  if constexpr (OP == ROW_SPLIT || OP == ROW_SPLIT_FIRST) {
+    if constexpr (OP == ROW_SPLIT) fft_line<Sh, true>(v, sm, t, tw, sync);
+    // psi = psi0 + delta with psi0 the probe's vacuum wave (shifted like the
+    // probe) and t = 1 + tau.  The reference's update (adfstem.cpp:1929-1949)
+    //   re' = (tr*re - ti*im)/s,  im' = (tr*im + ti*re')/s
+    // is linear over the reals, so the scattered part evolves as
+    //   dre' = (tau_r*p0r - ti*p0i + (1+tau_r)*dre - ti*dim)/s
+    //   dim' = (tau_r*p0i + (1+tau_r)*dim + ti*(p0r/s + dre'))/s
+    // and every term is formed at the scale of delta, not of psi0.
+    const int sx = a.shifts[2 * b], sy = a.shifts[2 * b + 1];
+    const int ix = (i < sx) ? i + a.nx - sx : i - sx;
+    const C* prow = static_cast<const C*>(a.psi0) + (int64_t)ix * N;
+    const C* trow = static_cast<const C*>(a.trans) + (int64_t)i * N;
+    const Real is = (Real)a.inv_s;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int y = t + T * m;
+      const int iy = (y < sy) ? y + N - sy : y - sy;
+      const C p0 = __ldg(prow + iy);
+      const C tau = __ldg(trow + y);
+      const C d = v[m];
+      const Real dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
+      const Real re_total = p0.x * is + dre;
+      const Real dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
+      v[m] = C{dre, dim};
+    }
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+  } else if constexpr (OP == ROW_FWD) {
     fft_line<Sh, false>(v, sm, t, tw, sync);
   } else if constexpr (OP == ROW_INV) {
     fft_line<Sh, true>(v, sm, t, tw, sync);
@@ -370,19 +400,43 @@ __global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__
 }
 
 // ------------------------------------------------------- detection -------
+// Value of one probe's exit wave at k-space pixel `pix`: the buffer value,
+// plus (split-wave runs) the vacuum part shifted to the probe's position.
+template <typename Real>
+__device__ __forceinline__ double2 exit_value(const Cx<Real>* __restrict__ p, int pix,
+                                              const SplitK& sk, int sx, int sy) {
+  const Cx<Real> v = p[pix];
+  double x = (double)v.x, y = (double)v.y;
+  if (sk.psi0k) {
+    const double2 z = __ldg(reinterpret_cast<const double2*>(sk.psi0k) + pix);
+    if (z.x != 0.0 || z.y != 0.0) {
+      const int mx = pix / sk.ny, my = pix - mx * sk.ny;
+      // e^{-2 pi i (mx sx / nx + my sy / ny)} from exact integer phases
+      const double f = (double)(((int64_t)mx * sx) % sk.nx) / sk.nx +
+                       (double)(((int64_t)my * sy) % sk.ny) / sk.ny;
+      double sn, cs;
+      sincospi(-2.0 * f, &sn, &cs);
+      x += z.x * cs - z.y * sn;
+      y += z.x * sn + z.y * cs;
+    }
+  }
+  return make_double2(x, y);
+}
+
 template <typename Real>
 __global__ void segment_sums_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
                                     const int32_t* __restrict__ idx,
                                     const int32_t* __restrict__ start, int ng,
-                                    double* amp, double* inten) {
+                                    double* amp, double* inten, const SplitK sk) {
   __shared__ double ra[32], ri[32];
   const int g = blockIdx.x, b = blockIdx.y;
   const Cx<Real>* p = psi + (int64_t)b * stride;
+  const int sx = sk.psi0k ? sk.shifts[2 * b] : 0, sy = sk.psi0k ? sk.shifts[2 * b + 1] : 0;
   double sa = 0.0, si = 0.0;
   const int s0 = start[g], s1 = start[g + 1];
   for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
-    const Cx<Real> v = p[idx[k]];
-    const double x = (double)v.x, y = (double)v.y;
+    const double2 v = exit_value<Real>(p, idx[k], sk, sx, sy);
+    const double x = v.x, y = v.y;
     const double i2 = x * x + y * y;
     si += i2;
     sa += sqrt(i2);
@@ -413,19 +467,34 @@ __global__ void segment_sums_kernel(const Cx<Real>* __restrict__ psi, int64_t st
 
 template <typename Real>
 __global__ void pixel_accum_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
-                                   int nb, int64_t npix, double* acc_a, double* acc_i) {
+                                   int nb, int64_t npix, double* acc_a, double* acc_i,
+                                   const SplitK sk) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npix) return;
   double sa = acc_a[p], si = acc_i[p];
   for (int b = 0; b < nb; ++b) {
-    const Cx<Real> v = psi[(int64_t)b * stride + p];
-    const double x = (double)v.x, y = (double)v.y;
+    const int sx = sk.psi0k ? sk.shifts[2 * b] : 0, sy = sk.psi0k ? sk.shifts[2 * b + 1] : 0;
+    const double2 v = exit_value<Real>(psi + (int64_t)b * stride, (int)p, sk, sx, sy);
+    const double x = v.x, y = v.y;
     const double i2 = x * x + y * y;
     sa += sqrt(i2);
     si += i2;
   }
   acc_a[p] = sa;
   acc_i[p] = si;
+}
+
+__global__ void to_f32_minus_one_kernel(const double2* __restrict__ in, float2* __restrict__ out,
+                                        int64_t n) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = make_float2((float)(in[k].x - 1.0), (float)in[k].y);
+}
+
+__global__ void assemble_split_kernel(const float2* __restrict__ delta, SplitK sk,
+                                      int32_t sx, int32_t sy, double2* out) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= (int64_t)sk.nx * sk.ny) return;
+  out[p] = exit_value<float>(delta, (int)p, sk, sx, sy);
 }
 
 inline unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
@@ -448,6 +517,8 @@ cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s) {
     switch (op) {
       case ROW_SLICE: return row_dispatch<float, ROW_SLICE>(a, s);
       case ROW_SLICE_FIRST: return row_dispatch<float, ROW_SLICE_FIRST>(a, s);
+      case ROW_SPLIT: return row_dispatch<float, ROW_SPLIT>(a, s);
+      case ROW_SPLIT_FIRST: return row_dispatch<float, ROW_SPLIT_FIRST>(a, s);
       default: return cudaErrorInvalidValue;  // set-up transforms run in FP64
     }
   }
@@ -532,26 +603,45 @@ cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t 
 
 cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t stride, int nb,
                                 const int32_t* idx, const int32_t* start, int ng,
-                                double* amp, double* inten, cudaStream_t s) {
+                                double* amp, double* inten, const SplitK& sk, cudaStream_t s) {
   if (ng <= 0 || nb <= 0) return cudaSuccess;
   dim3 grid(ng, nb);
   if (fp64)
     segment_sums_kernel<double><<<grid, 256, 0, s>>>(
-        static_cast<const double2*>(psi), stride, idx, start, ng, amp, inten);
+        static_cast<const double2*>(psi), stride, idx, start, ng, amp, inten, sk);
   else
     segment_sums_kernel<float><<<grid, 256, 0, s>>>(
-        static_cast<const float2*>(psi), stride, idx, start, ng, amp, inten);
+        static_cast<const float2*>(psi), stride, idx, start, ng, amp, inten, sk);
   return cudaGetLastError();
 }
 
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t stride, int nb,
-                               int64_t npix, double* acc_a, double* acc_i, cudaStream_t s) {
+                               int64_t npix, double* acc_a, double* acc_i, const SplitK& sk,
+                               cudaStream_t s) {
   if (fp64)
     pixel_accum_kernel<double><<<blocks_for(npix, 256), 256, 0, s>>>(
-        static_cast<const double2*>(psi), stride, nb, npix, acc_a, acc_i);
+        static_cast<const double2*>(psi), stride, nb, npix, acc_a, acc_i, sk);
   else
     pixel_accum_kernel<float><<<blocks_for(npix, 256), 256, 0, s>>>(
-        static_cast<const float2*>(psi), stride, nb, npix, acc_a, acc_i);
+        static_cast<const float2*>(psi), stride, nb, npix, acc_a, acc_i, sk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_f32_minus_one(const double* in, float* out, int64_t n, cudaStream_t s) {
+  to_f32_minus_one_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      reinterpret_cast<const double2*>(in), reinterpret_cast<float2*>(out), n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assemble_split(const float* delta, const double* psi0k, int nx, int ny,
+                                  int sx, int sy, double* out, cudaStream_t s) {
+  SplitK sk;
+  sk.psi0k = psi0k;
+  sk.nx = nx;
+  sk.ny = ny;
+  const int64_t n = (int64_t)nx * ny;
+  assemble_split_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      reinterpret_cast<const float2*>(delta), sk, sx, sy, reinterpret_cast<double2*>(out));
   return cudaGetLastError();
 }
 

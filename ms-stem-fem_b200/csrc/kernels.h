@@ -13,6 +13,12 @@ enum RowOp : int {
   ROW_INV = 1,          // inverse DFT along y, then * scale
   ROW_SLICE = 2,        // inverse DFT, transmission multiply, forward DFT
   ROW_SLICE_FIRST = 3,  // place shifted probe, transmission multiply, fwd DFT
+  // Split-wave slice passes (FP32): the buffer holds only the scattered part
+  // delta = psi - psi0 of each probe's wave, where psi0 is the probe's
+  // vacuum evolution (precomputed in FP64, shared by all probes up to an
+  // integer shift) and the transmission is stored as tau = t - 1.
+  ROW_SPLIT = 4,        // iDFT, delta' = Q(t, psi0 + delta) - psi0/s, DFT
+  ROW_SPLIT_FIRST = 5,  // delta = 0 on entry: delta' = Q(t, psi0) - psi0/s
 };
 // Which fused operation a column pass (transform along x, strided) does.
 enum ColOp : int {
@@ -41,6 +47,19 @@ struct PassArgs {
   const int32_t* mask_hi = nullptr;
   const void* px = nullptr;       // [nx] complex propagator along x (Real2)
   const void* py = nullptr;       // [ny] complex propagator along y (Real2)
+  // split-wave row passes: vacuum wave entering this slice, [nx][ny]
+  // complex, in the same scale as the inverse-transformed buffer
+  const void* psi0 = nullptr;
+};
+
+// Vacuum part of the exit wave for split-wave detection: k-space values of
+// the unshifted probe's vacuum exit wave (FP64, zero outside the aperture)
+// and per-probe pixel shifts; each probe adds psi0k[m] * e^{-2 pi i
+// (mx sx / nx + my sy / ny)} to its scattered part before |psi| is taken.
+struct SplitK {
+  const double* psi0k = nullptr;   // [nx][ny] complex; nullptr: not split
+  const int32_t* shifts = nullptr; // [nb][2]
+  int nx = 0, ny = 0;
 };
 
 // Returns false if the length is not supported.
@@ -82,10 +101,19 @@ cudaError_t launch_to_f32(const double* in, float* out, int64_t n_real,
 // sum |psi|^2 over pixel list idx[start[g] .. start[g+1]), FP64.
 cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t batch_stride,
                                 int nb, const int32_t* idx, const int32_t* start,
-                                int ng, double* amp, double* inten, cudaStream_t s);
+                                int ng, double* amp, double* inten, const SplitK& sk,
+                                cudaStream_t s);
 // acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
                                int nb, int64_t npix, double* acc_a, double* acc_i,
-                               cudaStream_t s);
+                               const SplitK& sk, cudaStream_t s);
+// out = (float)(in - 1) for the real parts, (float)in for the imaginary
+// parts of n complex doubles: tau = t - 1 for split-wave passes.
+cudaError_t launch_to_f32_minus_one(const double* in, float* out, int64_t n_complex,
+                                    cudaStream_t s);
+// psi (complex) = delta (FP32, k-space) + shifted vacuum part (FP64), for
+// one probe: used to return the exit wave of a split-wave run.
+cudaError_t launch_assemble_split(const float* delta, const double* psi0k, int nx, int ny,
+                                  int sx, int sy, double* out, cudaStream_t s);
 
 }  // namespace msf

@@ -84,6 +84,7 @@ class Results(C.Structure):
                 ("k_lower", _dp), ("bin_counts", _ip), ("v_omega", _dp), ("vbar_r", _dp),
                 ("v_re", _dp), ("omega_vimage", _dp), ("v_gt17", _dp), ("v_rbar", _dp),
                 ("final_psi", _dp), ("mean_amplitude", _dp), ("mean_intensity", _dp),
+                ("ring_amplitude", _dp), ("ring_intensity", _dp),
                 ("probe_slices", C.c_int64), ("kernel_launches", C.c_int64),
                 ("seconds_setup", C.c_double),
                 ("seconds_raster", C.c_double)]
@@ -266,10 +267,13 @@ class Context:
         return Specimen(self, grid, q, z)
 
     def run(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
-            want_final_psi=False, want_means=False, cap_k=8192) -> "RunResult":
+            want_final_psi=False, want_means=False, want_rings=False,
+            cap_k=8192) -> "RunResult":
         nx, ny = spec.grid.nx, spec.grid.ny
         n_r = raster.n_x * raster.n_y
-        out = RunResult(n_r, cap_k, nx, ny, want_final_psi, want_means)
+        if want_rings:
+            cap_k = min(cap_k, 1024)
+        out = RunResult(n_r, cap_k, nx, ny, want_final_psi, want_means, want_rings)
         _check(lib().msf_run(self._h, spec._h, C.byref(optics), C.byref(raster),
                              C.byref(detect), C.byref(out._struct)))
         out.finish(raster, detect)
@@ -328,7 +332,7 @@ class Specimen:
 
 
 class RunResult:
-    def __init__(self, n_r, cap_k, nx, ny, want_psi, want_means):
+    def __init__(self, n_r, cap_k, nx, ny, want_psi, want_means, want_rings=False):
         self.adf_image = np.zeros(n_r)
         self.k_lower = np.zeros(cap_k)
         self.bin_counts = np.zeros(cap_k, dtype=np.int32)
@@ -348,6 +352,13 @@ class RunResult:
         if want_means:
             s.mean_amplitude = _p(self.mean_amplitude)
             s.mean_intensity = _p(self.mean_intensity)
+        self.ring_amp = np.zeros(n_r * cap_k) if want_rings else None
+        self.ring_int = np.zeros(n_r * cap_k) if want_rings else None
+        if want_rings:
+            s.ring_amplitude = _p(self.ring_amp)
+            s.ring_intensity = _p(self.ring_int)
+        self._cap_k = cap_k
+        self._n_r = n_r
         self._struct = s
         self._shape = (nx, ny)
 
@@ -361,6 +372,9 @@ class RunResult:
         self.v = {m: self._v[m][:self.n_k] for m in FEM_MODES if detect.outputs & FEM_MODES[m]}
         self.k = self.k_lower[:self.n_k]
         self.counts = self.bin_counts[:self.n_k]
+        if self.ring_amp is not None:
+            self.rings_amp = self.ring_amp.reshape(self._n_r, self._cap_k)[:, :self.n_k]
+            self.rings_int = self.ring_int.reshape(self._n_r, self._cap_k)[:, :self.n_k]
         if self.final_psi is not None:
             self.final_psi_2d = self.final_psi.reshape(*self._shape, 2)
 
