@@ -212,6 +212,9 @@ def main():
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--raster", type=int, default=0,
+                    help="probes per raster side (default 64, the workload's); smaller "
+                         "values make a short case for profiling")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -232,6 +235,8 @@ def main():
     spec_path = work / "c2.data"
     make_specimen(spec_path)
     argv = ["-a", str(spec_path), "--output_prefix", str(work / "c2")] + WORKLOAD["argv"].split()
+    if args.raster:
+        argv[argv.index("--rasterspacing") + 1] = repr(WORKLOAD["box"][0] / args.raster)
     job = msf.Job(argv)
     q, z = job.positions()
     ctx = msf.Context(device=local, precision=args.precision, batch=args.batch,
