@@ -172,6 +172,18 @@ msf_status msf_run(msf_context* ctx, const msf_specimen* spec,
 msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
                      const msf_optics* optics, double* out);
 
+/* The probe of msf_probe written into caller-provided device memory
+ * (2*nx*ny doubles) on `stream` (a cudaStream_t, NULL for the default
+ * stream), allocating no device memory.  No counterpart in the reference.
+ * For callers that may not call cudaMalloc (an application that owns all
+ * device memory in its own pool, a running loop that must not stall on an
+ * allocation).  Its scratch is one fixed device array per device, sized for
+ * grids of at most 2048 x 2048; larger grids return MSF_ERR_ARG.  The first
+ * call on a device looks up that array's address and should come before any
+ * stream capture; calls that overlap on the GPU share the array and race. */
+msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
+                             double* probe_device, void* stream);
+
 /* ---- host-side set-up helpers (bit-exact with the reference) ----------- */
 /* lambda [A] and gamma for an accelerating voltage (tem.cpp:424-438). */
 void msf_wavelength(double voltage, double* lambda, double* gamma);

@@ -39,7 +39,7 @@ EXPORTED = [
     "msf_probe_shifts", "msf_ring_bins", "msf_parse_cmdline",
     "msf_job_destroy", "msf_job_describe", "msf_job_output_prefix",
     "msf_read_specimen", "msf_write_outputs", "msf_main", "msf_slice_atoms",
-    "msf_time_passes", "msf_context_transfer_bytes",
+    "msf_time_passes", "msf_context_transfer_bytes", "msf_probe_noalloc",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -141,6 +141,8 @@ def lib() -> C.CDLL:
         L.msf_slice_atoms.argtypes = [C.c_int64, _dp, C.c_double, C.c_double, C.c_double,
                                       _ip, _dp, _dp, _lp, _lp, C.c_int32]
         L.msf_context_transfer_bytes.argtypes = [C.c_void_p, _lp, _lp, C.c_int32]
+        L.msf_probe_noalloc.argtypes = [C.POINTER(Grid), C.POINTER(Optics), C.c_void_p,
+                                        C.c_void_p]
         L.msf_time_passes.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]
         _lib = L
     return _lib
