@@ -42,6 +42,14 @@ template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) 
 
 template <int I> using ic = std::integral_constant<int, I>;
 
+// Loads issued between two fences may be scheduled together; a fence keeps
+// later loads from being hoisted above it (register pressure control).
+#ifndef MSF_LOAD_CHUNK
+#define MSF_LOAD_CHUNK 8
+#endif
+constexpr int kLoadChunk = MSF_LOAD_CHUNK;
+__device__ __forceinline__ void load_fence() { asm volatile("" ::: "memory"); }
+
 // Compile-time loop: f(ic<B>), f(ic<B+S>), ... while < E.
 template <int B, int E, int S = 1, typename F>
 __device__ __forceinline__ void sfor(F&& f) {
@@ -126,9 +134,18 @@ template <int N, typename Real> struct Shape;
 MSF_SHAPE(64, float, 8, 2, 8, 8, 1)
 MSF_SHAPE(128, float, 16, 2, 16, 8, 1)
 MSF_SHAPE(256, float, 16, 2, 16, 16, 1)
+#ifndef MSF_F32_WIDE
+#define MSF_F32_WIDE 1
+#endif
+#if MSF_F32_WIDE
 MSF_SHAPE(512, float, 32, 2, 32, 16, 1)
 MSF_SHAPE(1024, float, 32, 2, 32, 32, 1)
 MSF_SHAPE(2048, float, 32, 3, 32, 8, 8)
+#else
+MSF_SHAPE(512, float, 16, 3, 16, 16, 2)
+MSF_SHAPE(1024, float, 16, 3, 16, 16, 4)
+MSF_SHAPE(2048, float, 16, 3, 16, 16, 8)
+#endif
 MSF_SHAPE(4096, float, 16, 3, 16, 16, 16)
 MSF_SHAPE(64, double, 8, 2, 8, 8, 1)
 MSF_SHAPE(128, double, 16, 2, 16, 8, 1)
@@ -139,12 +156,62 @@ MSF_SHAPE(2048, double, 16, 3, 16, 16, 8)
 MSF_SHAPE(4096, double, 16, 3, 16, 16, 16)
 #undef MSF_SHAPE
 
+// Worst bank multiplicity of one shared-memory access phase (128 bytes of
+// lanes) over the exchanges of a line FFT, for lines `stride` elements
+// apart.  Lanes are numbered lane = line_fast ? line + LINES*t : t + T*line;
+// `line_fast` is the column pass's thread order (column index fastest).
+template <class Sh, int ELEM_BYTES>
+constexpr int bank_conflicts(int stride, int lines, bool line_fast) {
+  const int P = 128 / ELEM_BYTES;           // lanes per conflict-free phase
+  const int units = 128 / ELEM_BYTES;       // distinct bank slots per phase
+  const int shift = ilog2(Sh::R0);
+  int worst = 1;
+  for (int s = 0; s + 1 < Sh::S; ++s) {     // exchange after stage s
+    const int R = Sh::radix(s), NB = Sh::E / R, NS = Sh::ns(s);
+    const int R2 = Sh::radix(s + 1), NB2 = Sh::E / R2;
+    for (int pass = 0; pass < 2; ++pass) {  // 0: writes, 1: reads of next stage
+      const int cnt_b = pass == 0 ? NB : NB2, cnt_r = pass == 0 ? R : R2;
+      for (int b = 0; b < cnt_b; ++b)
+        for (int r = 0; r < cnt_r; ++r) {
+          int hits[32] = {};
+          for (int lane = 0; lane < P; ++lane) {
+            const int line = line_fast ? lane % lines : (Sh::T >= P ? 0 : lane / Sh::T);
+            const int t = line_fast ? lane / lines : (Sh::T >= P ? lane : lane % Sh::T);
+            const int j = t + Sh::T * b;
+            const int a = pass == 0 ? (j / NS) * NS * R + (j % NS) + r * NS
+                                    : j + r * (Sh::N / R2);
+            const int addr = line * stride + a + (a >> shift);
+            const int u = addr % units;
+            hits[u] += 1;
+            if (hits[u] > worst) worst = hits[u];
+          }
+        }
+    }
+  }
+  return worst;
+}
+
+// Line stride (elements) with the fewest bank conflicts among the
+// candidates base .. base + 16 (base = N plus one padding slot every R0).
+template <class Sh, int ELEM_BYTES, int LINES, bool LINE_FAST>
+constexpr int best_stride() {
+  const int base = Sh::N + (Sh::N >> ilog2(Sh::R0));
+  int best = base + 1, best_c = 1 << 30;
+  for (int k = 0; k <= 16; ++k) {
+    const int c = bank_conflicts<Sh, ELEM_BYTES>(base + k, LINES, LINE_FAST);
+    if (c < best_c) { best_c = c; best = base + k; }
+  }
+  return best;
+}
+
 // Shared-memory line layout: one padding slot every R0 elements keeps the
-// stride-R0 writes of the first exchange conflict-free; the odd line stride
-// keeps neighbouring lines (columns) on different banks.
-template <class Sh> struct Smem {
+// stride-R0 writes of the first exchange conflict-free; the line stride is
+// chosen so lines sharing an access phase (columns of a column pass, short
+// rows of a row pass) fall on different banks.
+template <class Sh, int ELEM_BYTES = 8, int LINES = 1, bool LINE_FAST = false>
+struct Smem {
   static constexpr int pad_shift = ilog2(Sh::R0);
-  static constexpr int stride = Sh::N + (Sh::N >> pad_shift) + 1;
+  static constexpr int stride = best_stride<Sh, ELEM_BYTES, LINES, LINE_FAST>();
   __device__ __forceinline__ static int at(int a) { return a + (a >> pad_shift); }
 };
 
@@ -180,6 +247,9 @@ __device__ __forceinline__ void fft_line(C (&v)[Sh::E], C* __restrict__ sm,
         const int k = j & (NS - 1);
         sfor<1, R>([&](auto rI) {
           constexpr int r = decltype(rI)::value;
+          // keep at most kLoadChunk table loads in flight: bounds the
+          // registers the compiler spends on hoisted twiddles
+          if constexpr (r % kLoadChunk == 0) load_fence();
           const C w = __ldg(&tw[r * k * (N / (NS * R))]);
           v[b + r * NB] = INV ? cmulc(v[b + r * NB], w) : cmul(v[b + r * NB], w);
         });

@@ -26,32 +26,55 @@ namespace {
 constexpr double kRefPi = 3.14159265369;  // the reference's PI (adfstem.hpp:55)
 constexpr int kSmemBudget = 220 * 1024;
 
+#ifndef MSF_ROW_THREADS
+#define MSF_ROW_THREADS 256
+#endif
+#ifndef MSF_COL_THREADS
+#define MSF_COL_THREADS 256
+#endif
+
+#ifndef MSF_THREADS_PER_SM
+#define MSF_THREADS_PER_SM 256
+#endif
+// Resident CTAs per SM the register allocator must allow, so that at least
+// MSF_THREADS_PER_SM threads of a pass share an SM.
+constexpr int min_blocks(int real_bytes, int threads) {
+  if (real_bytes == 8) return 1;  // FP64 passes keep their registers
+  return threads >= MSF_THREADS_PER_SM ? 1 : MSF_THREADS_PER_SM / threads;
+}
+
+// Lines (rows) per CTA of a row pass: about MSF_ROW_THREADS threads, small
+// CTAs so that several reside per SM and their load / FFT / store phases
+// overlap.
 template <typename Real, int N>
 constexpr int row_lines() {
   using Sh = Shape<N, Real>;
-  constexpr int bytes = Smem<Sh>::stride * (int)sizeof(Cx<Real>);
-  int l = 256 / Sh::T;
+  constexpr int bytes = (Sh::N + (Sh::N >> ilog2(Sh::R0)) + 16) * (int)sizeof(Cx<Real>);
+  int l = MSF_ROW_THREADS / Sh::T;
   if (l < 1) l = 1;
   while (l > 1 && l * bytes > kSmemBudget) l >>= 1;
   return l;
 }
 
+// Columns per CTA of a column pass: as many as fit MSF_COL_THREADS threads
+// (16 FP32 / 8 FP64 columns give 128-byte row segments).
 template <typename Real, int N>
 constexpr int col_cols() {
   using Sh = Shape<N, Real>;
-  constexpr int bytes = Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  constexpr int bytes = (Sh::N + (Sh::N >> ilog2(Sh::R0)) + 16) * (int)sizeof(Cx<Real>);
   int c = sizeof(Real) == 4 ? 16 : 8;
-  while (c > 1 && (c * bytes > kSmemBudget || c * Sh::T > 256)) c >>= 1;
+  while (c > 1 && (c * bytes > kSmemBudget || c * Sh::T > MSF_COL_THREADS)) c >>= 1;
   return c;
 }
 
 // ------------------------------------------------------------ row pass ---
 template <typename Real, int N, int LINES, int OP>
-__global__ void __launch_bounds__(LINES * Shape<N, Real>::T)
+__global__ void __launch_bounds__(LINES * Shape<N, Real>::T,
+                                  min_blocks((int)sizeof(Real), LINES * Shape<N, Real>::T))
 row_kernel(const PassArgs a) {
   using C = Cx<Real>;
   using Sh = Shape<N, Real>;
-  using SM = Smem<Sh>;
+  using SM = Smem<Sh, (int)sizeof(Cx<Real>), LINES, false>;
   constexpr int E = Sh::E, T = Sh::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
@@ -101,6 +124,7 @@ row_kernel(const PassArgs a) {
     const Real is = (Real)a.inv_s;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
+      if (m % kLoadChunk == 0) load_fence();
       const int y = t + T * m;
       const int iy = (y < sy) ? y + N - sy : y - sy;
       const C p0 = __ldg(prow + iy);
@@ -127,6 +151,7 @@ row_kernel(const PassArgs a) {
     const Real is = (Real)a.inv_s;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
+      if (m % kLoadChunk == 0) load_fence();
       const C tv = __ldg(trow + t + T * m);
       const Real re = (tv.x * v[m].x - tv.y * v[m].y) * is;
       const Real im = (tv.x * v[m].y + tv.y * re) * is;
@@ -140,11 +165,12 @@ row_kernel(const PassArgs a) {
 
 // --------------------------------------------------------- column pass ---
 template <typename Real, int N, int COLS, int OP>
-__global__ void __launch_bounds__(COLS * Shape<N, Real>::T)
+__global__ void __launch_bounds__(COLS * Shape<N, Real>::T,
+                                  min_blocks((int)sizeof(Real), COLS * Shape<N, Real>::T))
 col_kernel(const PassArgs a) {
   using C = Cx<Real>;
   using Sh = Shape<N, Real>;
-  using SM = Smem<Sh>;
+  using SM = Smem<Sh, (int)sizeof(Cx<Real>), COLS, true>;
   constexpr int E = Sh::E, T = Sh::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* smem = reinterpret_cast<C*>(smem_raw);
@@ -181,6 +207,7 @@ col_kernel(const PassArgs a) {
         const C* px = static_cast<const C*>(a.px);
 #pragma unroll
         for (int m = 0; m < E; ++m) {
+          if (m % kLoadChunk == 0) load_fence();
           const int i = t + T * m;
           if (i < lo || i >= hi) {
             const C p = cmul(__ldg(px + i), pyj);  // slice.cpp:1396-1412
@@ -202,7 +229,7 @@ template <typename Real, int N, int OP>
 cudaError_t row_launch(const PassArgs& a, cudaStream_t s) {
   constexpr int L = row_lines<Real, N>();
   using Sh = Shape<N, Real>;
-  constexpr int smem = L * Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  constexpr int smem = L * Smem<Sh, (int)sizeof(Cx<Real>), L, false>::stride * (int)sizeof(Cx<Real>);
   static bool configured = false;
   auto k = row_kernel<Real, N, L, OP>;
   if (!configured) {
@@ -220,7 +247,7 @@ template <typename Real, int N, int OP>
 cudaError_t col_launch(const PassArgs& a, cudaStream_t s) {
   constexpr int CC = col_cols<Real, N>();
   using Sh = Shape<N, Real>;
-  constexpr int smem = CC * Smem<Sh>::stride * (int)sizeof(Cx<Real>);
+  constexpr int smem = CC * Smem<Sh, (int)sizeof(Cx<Real>), CC, true>::stride * (int)sizeof(Cx<Real>);
   static bool configured = false;
   auto k = col_kernel<Real, N, CC, OP>;
   if (!configured) {
