@@ -1,4 +1,5 @@
 // extern "C" entry points of libmsf.so (declared in include/msf.h).
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -75,6 +76,7 @@ msf_status msf_context_create(const msf_options* opt, msf_context** out) {
   c->fp64 = o.precision == MSF_FP64;
   c->batch = o.batch;
   c->graphs = o.use_graphs != 0;
+  if (const char* p = std::getenv("MSF_PIPE")) c->pipe = std::atoi(p);
   c->budget = o.hbm_budget;
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {

@@ -362,20 +362,43 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   col.mask_hi = spec->mask_hi.as<int32_t>();
   col.px = spec->prop.p;
   col.py = static_cast<const char*>(spec->prop.p) + cbytes * g.nx;
+  // the same kernels run_raster launches for slices after the first
+  const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
+  const bool pipe_row = pipe_ok && (ctx->pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_ok && (ctx->pipe & MSF_PIPE_COL);
+  alignas(64) unsigned char col_map[128];
+  DevBuf d_err;
+  MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
+  MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
+  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, nb, g.nx, g.ny, col_map));
+  auto row_pass = [&]() {
+    return pipe_row ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
+                    : launch_row(fp64, rop, row, ctx->stream);
+  };
+  auto col_pass = [&]() {
+    return pipe_col ? launch_col_slice_pipe(col, false, col_map, d_err.as<int>(), ctx->stream)
+                    : launch_col(fp64, COL_SLICE, col, ctx->stream);
+  };
   std::vector<cudaEvent_t> ev(2 * reps + 2);
   for (auto& e : ev) MSF_CUDA(cudaEventCreate(&e));
   // warm-up
-  MSF_CUDA(launch_row(fp64, rop, row, ctx->stream));
-  MSF_CUDA(launch_col(fp64, COL_SLICE, col, ctx->stream));
+  MSF_CUDA(row_pass());
+  MSF_CUDA(col_pass());
   double tr = 0, tc = 0;
   for (int r = 0; r < reps; ++r) {
     MSF_CUDA(cudaEventRecord(ev[2 * r], ctx->stream));
-    MSF_CUDA(launch_row(fp64, rop, row, ctx->stream));
+    MSF_CUDA(row_pass());
     MSF_CUDA(cudaEventRecord(ev[2 * r + 1], ctx->stream));
-    MSF_CUDA(launch_col(fp64, COL_SLICE, col, ctx->stream));
+    MSF_CUDA(col_pass());
     MSF_CUDA(cudaEventRecord(ev[2 * r + 2], ctx->stream));
   }
   MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  int err_flag = 0;
+  MSF_CUDA(cudaMemcpy(&err_flag, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err_flag) {
+    set_error("a pipelined slice pass gave up waiting for a tile copy (bounded wait)");
+    return MSF_ERR_TIMEOUT;
+  }
   for (int r = 0; r < reps; ++r) {
     float a = 0, b = 0;
     MSF_CUDA(cudaEventElapsedTime(&a, ev[2 * r], ev[2 * r + 1]));
@@ -505,6 +528,16 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   DevBuf psi;
   MSF_TRY(ctx->alloc(&psi, cbytes * plane * B));
 
+  // persistent TMA-pipelined passes for FP32 grids they support
+  const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
+  const bool pipe_row = pipe_ok && (ctx->pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_ok && (ctx->pipe & MSF_PIPE_COL);
+  alignas(64) unsigned char col_map[128];
+  DevBuf d_err;
+  MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
+  MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
+  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map));
+
   PassArgs row, col;
   row.psi = col.psi = psi.p;
   row.batch_stride = col.batch_stride = plane;
@@ -535,10 +568,16 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
         op = s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT;
         row.psi0 = psi0_tab.as<float>() + 2 * plane * s;
       }
-      MSF_CUDA(launch_row(fp64, op, row, ctx->stream));
+      if (pipe_row && op == ROW_SPLIT)
+        MSF_CUDA(launch_row_split_pipe(row, d_err.as<int>(), ctx->stream));
+      else
+        MSF_CUDA(launch_row(fp64, op, row, ctx->stream));
       col.px = pbase + prop_stride * s;
       col.py = pbase + prop_stride * s + cbytes * g.nx;
-      MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
+      if (pipe_col)
+        MSF_CUDA(launch_col_slice_pipe(col, s + 1 == S, col_map, d_err.as<int>(), ctx->stream));
+      else
+        MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
     }
     SplitK sk;
     if (!fp64) {
@@ -636,6 +675,12 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     }
   }
   MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  int err_flag = 0;
+  MSF_CUDA(cudaMemcpy(&err_flag, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err_flag) {
+    set_error("a pipelined slice pass gave up waiting for a tile copy (bounded wait)");
+    return MSF_ERR_TIMEOUT;
+  }
   float ms = 0;
   MSF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   cudaEventDestroy(ev0);

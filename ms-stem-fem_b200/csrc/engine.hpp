@@ -37,11 +37,16 @@ struct DevBuf {
 
 }  // namespace msf
 
+constexpr int MSF_PIPE_COL = 1, MSF_PIPE_ROW = 2;
+
 struct msf_context {
   int device = 0;
   bool fp64 = true;
   int batch = 0;
   bool graphs = true;
+  // persistent TMA-pipelined FP32 passes: bit mask of MSF_PIPE_COL and
+  // MSF_PIPE_ROW, overridden by the MSF_PIPE environment variable
+  int pipe = MSF_PIPE_COL;
   int64_t budget = 0;
   int64_t allocated = 0;
   int64_t h2d_bytes = 0, d2h_bytes = 0;

@@ -1,0 +1,388 @@
+// Persistent, TMA-pipelined versions of the two FP32 slice passes.
+//
+// One CTA per SM walks a list of work items (a group of rows, or a group of
+// columns, of one probe).  While it transforms item k out of one shared
+// buffer, the tensor-memory accelerator already copies item k+1 into the
+// other: rows arrive as 1-D bulk copies (cp.async.bulk), column tiles as
+// 2-D tiled copies through a tensor map (cp.async.bulk.tensor), both
+// completing on an mbarrier.  The transform itself is the same register
+// Stockham FFT as kernels.cu; the buffer that just delivered the item also
+// serves as the exchange buffer.
+//
+// Every wait is bounded: if an mbarrier phase does not complete within
+// kSpinLimit polls the CTA records an error in *err and leaves its loop,
+// first waiting (bounded again) for any copy it still has in flight.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "fft_core.cuh"
+#include "kernels.h"
+
+namespace msf {
+
+namespace {
+
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kSpinLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tile_g2s(void* dst, const CUtensorMap* map, int x, int y,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Thread 0 waits (bounded) for the buffer's phase, the CTA learns the
+// outcome through shared memory, then every thread observes the completed
+// phase itself (acquiring the copied data).
+__device__ __forceinline__ bool cta_wait(uint64_t* bar, uint32_t parity, int* flag_smem) {
+  if (threadIdx.x == 0) *flag_smem = mbar_wait_bounded(bar, parity) ? 1 : 0;
+  __syncthreads();
+  const bool ok = *flag_smem != 0;
+  if (ok) mbar_wait_bounded(bar, parity);
+  return ok;
+}
+
+// ------------------------------------------------------- row pass (split) --
+template <int N, int LINES>
+__global__ void __launch_bounds__(LINES * Shape<N, float>::T, 1)
+row_split_pipe_kernel(const PassArgs a, int* err) {
+  using C = float2;
+  using Sh = Shape<N, float>;
+  using SM = Smem<Sh, 8, LINES, false>;
+  constexpr int E = Sh::E, T = Sh::T;
+  static_assert(SM::stride % 2 == 0, "line starts must be 16-byte aligned for bulk copies");
+  constexpr int BUF = LINES * SM::stride;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C* bufs = reinterpret_cast<C*>(smem_raw);
+  __shared__ uint64_t bars[2];
+  __shared__ int flag;
+  const int line = threadIdx.x / T, t = threadIdx.x % T;
+  const int items = a.nb * (a.nx / LINES);
+  auto sync = [] {
+    if constexpr (T <= 32) __syncwarp();
+    else __syncthreads();
+  };
+  auto issue = [&](int item, int which) {
+    const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
+    const C* src = static_cast<const C*>(a.psi) + (int64_t)b * a.batch_stride +
+                   (int64_t)g * LINES * N;
+    C* dst = bufs + which * BUF;
+    mbar_expect_tx(&bars[which], LINES * N * 8);
+    for (int l = 0; l < LINES; ++l)
+      bulk_g2s(dst + l * SM::stride, src + (int64_t)l * N, N * 8, &bars[which]);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int item = blockIdx.x;
+  if (threadIdx.x == 0) {
+    if (item < items) issue(item, 0);
+    if (item + (int)gridDim.x < items) issue(item + gridDim.x, 1);
+  }
+  uint32_t parity[2] = {0, 0};
+  const C* tw = static_cast<const C*>(a.tw);
+  const float is = (float)a.inv_s;
+  int k = 0;
+  for (; item < items; ++k, item += gridDim.x) {
+    const int w = k & 1;
+    if (!cta_wait(&bars[w], parity[w], &flag)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        // the other buffer may still be receiving a copy: wait for it
+        if (item + (int)gridDim.x < items) mbar_wait_bounded(&bars[w ^ 1], parity[w ^ 1]);
+      }
+      return;
+    }
+    parity[w] ^= 1;
+    const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
+    const int i = g * LINES + line;
+    C* sm = bufs + w * BUF + line * SM::stride;
+    C v[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = sm[t + T * m];
+    sync();
+    fft_line<Sh, true>(v, sm, t, tw, sync);
+    // split-wave transmission update, as ROW_SPLIT in kernels.cu
+    const int sx = a.shifts[2 * b], sy = a.shifts[2 * b + 1];
+    const int ix = (i < sx) ? i + a.nx - sx : i - sx;
+    const C* prow = static_cast<const C*>(a.psi0) + (int64_t)ix * N;
+    const C* trow = static_cast<const C*>(a.trans) + (int64_t)i * N;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      if (m % kLoadChunk == 0) load_fence();
+      const int y = t + T * m;
+      const int iy = (y < sy) ? y + N - sy : y - sy;
+      const C p0 = __ldg(prow + iy);
+      const C tau = __ldg(trow + y);
+      const C d = v[m];
+      const float dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
+      const float re_total = p0.x * is + dre;
+      const float dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
+      v[m] = C{dre, dim};
+    }
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+    C* row = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)i * N;
+#pragma unroll
+    for (int m = 0; m < E; ++m) row[t + T * m] = v[m];
+    __syncthreads();
+    if (threadIdx.x == 0 && item + 2 * (int)gridDim.x < items) {
+      fence_proxy_async();
+      issue(item + 2 * gridDim.x, w);
+    }
+  }
+}
+
+// ----------------------------------------------------- column slice pass --
+template <int N, int COLS, bool LAST>
+__global__ void __launch_bounds__(COLS * Shape<N, float>::T, 1)
+col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap, int* err) {
+  using C = float2;
+  using Sh = Shape<N, float>;
+  using SM = Smem<Sh, 8, COLS, true>;
+  constexpr int E = Sh::E, T = Sh::T;
+  constexpr int BOX = N < 256 ? N : 256;
+  constexpr int RAW = (N * COLS > COLS * SM::stride ? N * COLS : COLS * SM::stride);
+  constexpr int BUF = (RAW + 15) / 16 * 16;  // 128-byte multiple
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C* bufs = reinterpret_cast<C*>(smem_raw);
+  __shared__ uint64_t bars[2];
+  __shared__ int flag;
+  const int c = threadIdx.x % COLS, t = threadIdx.x / COLS;
+  const int items = a.nb * (a.ny / COLS);
+  auto sync = [] { __syncthreads(); };
+  auto issue = [&](int item, int which) {
+    const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
+    C* dst = bufs + which * BUF;
+    mbar_expect_tx(&bars[which], N * COLS * 8);
+#pragma unroll
+    for (int q = 0; q < N / BOX; ++q)
+      tile_g2s(dst + q * BOX * COLS, &tmap, g * COLS, b * a.nx + q * BOX, &bars[which]);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int item = blockIdx.x;
+  if (threadIdx.x == 0) {
+    if (item < items) issue(item, 0);
+    if (item + (int)gridDim.x < items) issue(item + gridDim.x, 1);
+  }
+  uint32_t parity[2] = {0, 0};
+  const C* tw = static_cast<const C*>(a.tw);
+  const float is = (float)a.inv_s;
+  const C* px = static_cast<const C*>(a.px);
+  int k = 0;
+  for (; item < items; ++k, item += gridDim.x) {
+    const int w = k & 1;
+    if (!cta_wait(&bars[w], parity[w], &flag)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        if (item + (int)gridDim.x < items) mbar_wait_bounded(&bars[w ^ 1], parity[w ^ 1]);
+      }
+      return;
+    }
+    parity[w] ^= 1;
+    const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
+    const int j = g * COLS + c;
+    C* base = bufs + w * BUF;
+    C v[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = base[(t + T * m) * COLS + c];
+    __syncthreads();
+    C* sm = base + c * SM::stride;
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+    const int lo = __ldg(a.mask_lo + j), hi = __ldg(a.mask_hi + j);
+    const C pyj = __ldg(static_cast<const C*>(a.py) + j);
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      if (m % kLoadChunk == 0) load_fence();
+      const int i = t + T * m;
+      if (i < lo || i >= hi) {
+        const C p = cmul(__ldg(px + i), pyj);
+        v[m] = cmul(p, cscale(v[m], is));
+      } else {
+        v[m] = C{0.f, 0.f};
+      }
+    }
+    if constexpr (!LAST) fft_line<Sh, true>(v, sm, t, tw, sync);
+    C* col = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + j;
+#pragma unroll
+    for (int m = 0; m < E; ++m) col[(int64_t)(t + T * m) * a.ny] = v[m];
+    __syncthreads();
+    if (threadIdx.x == 0 && item + 2 * (int)gridDim.x < items) {
+      fence_proxy_async();
+      issue(item + 2 * gridDim.x, w);
+    }
+  }
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+template <int N>
+constexpr int pipe_lines() { return 256 / Shape<N, float>::T; }
+template <int N>
+constexpr int pipe_cols() {
+  int c = 16;
+  while (c > 1 && c * Shape<N, float>::T > 256) c >>= 1;
+  return c;
+}
+
+template <int N>
+cudaError_t row_pipe_launch(const PassArgs& a, int* err, cudaStream_t s) {
+  constexpr int L = pipe_lines<N>();
+  using SM = Smem<Shape<N, float>, 8, L, false>;
+  constexpr int smem = 2 * L * SM::stride * 8;
+  static bool configured = false;
+  auto k = row_split_pipe_kernel<N, L>;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int items = a.nb * (a.nx / L);
+  const int grid = items < sm_count() ? items : sm_count();
+  k<<<grid, L * Shape<N, float>::T, smem, s>>>(a, err);
+  return cudaGetLastError();
+}
+
+template <int N, bool LAST>
+cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
+                            cudaStream_t s) {
+  constexpr int CC = pipe_cols<N>();
+  using SM = Smem<Shape<N, float>, 8, CC, true>;
+  constexpr int RAW = (N * CC > CC * SM::stride ? N * CC : CC * SM::stride);
+  constexpr int smem = 2 * ((RAW + 15) / 16 * 16) * 8;
+  static bool configured = false;
+  auto k = col_slice_pipe_kernel<N, CC, LAST>;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int items = a.nb * (a.ny / CC);
+  const int grid = items < sm_count() ? items : sm_count();
+  k<<<grid, CC * Shape<N, float>::T, smem, s>>>(a, map, err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool pipe_supported(int nx, int ny) {
+  auto ok = [](int n) { return n == 256 || n == 512 || n == 1024 || n == 2048; };
+  return ok(nx) && ok(ny);
+}
+
+int pipe_cols_for(int nx) {
+  switch (nx) {
+    case 256: return pipe_cols<256>();
+    case 512: return pipe_cols<512>();
+    case 1024: return pipe_cols<1024>();
+    case 2048: return pipe_cols<2048>();
+  }
+  return 0;
+}
+
+cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s) {
+  switch (a.ny) {
+    case 256: return row_pipe_launch<256>(a, err, s);
+    case 512: return row_pipe_launch<512>(a, err, s);
+    case 1024: return row_pipe_launch<1024>(a, err, s);
+    case 2048: return row_pipe_launch<2048>(a, err, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_col_slice_pipe(const PassArgs& a, bool last, const void* tensor_map,
+                                  int* err, cudaStream_t s) {
+  const CUtensorMap& m = *static_cast<const CUtensorMap*>(tensor_map);
+  switch (a.nx) {
+    case 256: return last ? col_pipe_launch<256, true>(a, m, err, s) : col_pipe_launch<256, false>(a, m, err, s);
+    case 512: return last ? col_pipe_launch<512, true>(a, m, err, s) : col_pipe_launch<512, false>(a, m, err, s);
+    case 1024: return last ? col_pipe_launch<1024, true>(a, m, err, s) : col_pipe_launch<1024, false>(a, m, err, s);
+    case 2048: return last ? col_pipe_launch<2048, true>(a, m, err, s) : col_pipe_launch<2048, false>(a, m, err, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// Tensor map over a batch of FP32 complex planes [nb*nx rows][ny columns],
+// 8-byte elements, box {cols, min(256, nx)} rows; no multicast, no swizzle.
+cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const int cols = pipe_cols_for(nx);
+  if (!cols) return cudaErrorInvalidValue;
+  cuuint64_t dims[2] = {(cuuint64_t)ny, (cuuint64_t)nx * (cuuint64_t)nb};
+  cuuint64_t strides[1] = {(cuuint64_t)ny * 8};
+  cuuint32_t box[2] = {(cuuint32_t)cols, (cuuint32_t)(nx < 256 ? nx : 256)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode(static_cast<CUtensorMap*>(map_out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, psi,
+                      dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+}  // namespace msf
