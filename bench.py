@@ -59,14 +59,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(name="row_col_pass_1024_fp32.md"):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/), or None before one was captured."""
+def ncu_traffic(which, name="row_col_pass_1024_fp32.md"):
+    """DRAM bytes per launch of the row or column pass ("row" / "col") from
+    the committed ncu summary (profiles/), or None before one was captured."""
     p = ROOT / "profiles" / name
     if not p.exists():
         return None
+    key = "traffic_bytes_per_launch_%s:" % which
     for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -282,7 +283,8 @@ def main():
     t_dom = max(ms_row, ms_col) * 1e-3
     peak, peak_kind = measured_peaks()
     achieved = alg / t_dom / 1e9
-    traffic = ncu_traffic()
+    # the ncu capture is at 1024^2 FP32 with 32 probes per launch
+    traffic = ncu_traffic(dom) if (n == 1024 and args.precision == "fp32" and nb == 32) else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "kernel": "%s pass (fused FFT + %s), %d probes/launch" %
