@@ -29,6 +29,12 @@ constexpr int kSmemBudget = 220 * 1024;
 #ifndef MSF_ROW_THREADS
 #define MSF_ROW_THREADS 256
 #endif
+// FP32 row passes hold 32 complex values per thread (one CTA of 256 threads
+// fills the register file): CTAs of 64 threads let four of them share an SM
+// with their load and transform phases out of step.
+#ifndef MSF_ROW_THREADS_F32
+#define MSF_ROW_THREADS_F32 64
+#endif
 #ifndef MSF_COL_THREADS
 #define MSF_COL_THREADS 256
 #endif
@@ -43,14 +49,14 @@ constexpr int min_blocks(int real_bytes, int threads) {
   return threads >= MSF_THREADS_PER_SM ? 1 : MSF_THREADS_PER_SM / threads;
 }
 
-// Lines (rows) per CTA of a row pass: about MSF_ROW_THREADS threads, small
-// CTAs so that several reside per SM and their load / FFT / store phases
-// overlap.
+// Lines (rows) per CTA of a row pass: about MSF_ROW_THREADS (FP64) or
+// MSF_ROW_THREADS_F32 threads, small CTAs so that several reside per SM and
+// their load / FFT / store phases overlap.
 template <typename Real, int N>
 constexpr int row_lines() {
   using Sh = Shape<N, Real>;
   constexpr int bytes = (Sh::N + (Sh::N >> ilog2(Sh::R0)) + 16) * (int)sizeof(Cx<Real>);
-  int l = MSF_ROW_THREADS / Sh::T;
+  int l = (sizeof(Real) == 4 ? MSF_ROW_THREADS_F32 : MSF_ROW_THREADS) / Sh::T;
   if (l < 1) l = 1;
   while (l > 1 && l * bytes > kSmemBudget) l >>= 1;
   return l;
