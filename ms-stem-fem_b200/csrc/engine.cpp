@@ -504,9 +504,20 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   seg_idx.insert(seg_idx.end(), adf_pix.begin(), adf_pix.end());
   seg_start.push_back((int32_t)seg_idx.size());
   const int n_seg = n_k + 1;
-  DevBuf d_seg_idx, d_seg_start, d_amp, d_int, d_acc_a, d_acc_i;
+  // chunks of at most kSegmentChunk pixels, never straddling two segments
+  std::vector<int32_t> chunk_begin, seg_chunk;
+  for (int gi = 0; gi < n_seg; ++gi) {
+    seg_chunk.push_back((int32_t)chunk_begin.size());
+    for (int32_t k = seg_start[gi]; k < seg_start[gi + 1]; k += kSegmentChunk)
+      chunk_begin.push_back(k);
+  }
+  seg_chunk.push_back((int32_t)chunk_begin.size());
+  const int n_chunks = (int)chunk_begin.size();
+  chunk_begin.push_back(seg_start[n_seg]);
+  DevBuf d_seg_idx, d_chunk_begin, d_seg_chunk, d_partial, d_amp, d_int, d_acc_a, d_acc_i;
   MSF_TRY(upload(ctx, &d_seg_idx, seg_idx));
-  MSF_TRY(upload(ctx, &d_seg_start, seg_start));
+  MSF_TRY(upload(ctx, &d_chunk_begin, chunk_begin));
+  MSF_TRY(upload(ctx, &d_seg_chunk, seg_chunk));
   MSF_TRY(ctx->alloc(&d_amp, sizeof(double) * n_probes * n_seg));
   MSF_TRY(ctx->alloc(&d_int, sizeof(double) * n_probes * n_seg));
   if (pix_modes) {
@@ -527,6 +538,14 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   B = (int)std::min<int64_t>(B, n_probes);
   DevBuf psi;
   MSF_TRY(ctx->alloc(&psi, cbytes * plane * B));
+  MSF_TRY(ctx->alloc(&d_partial, sizeof(double) * 2 * B * std::max(n_chunks, 1)));
+  SegmentPlan seg;
+  seg.idx = d_seg_idx.as<int32_t>();
+  seg.chunk_begin = d_chunk_begin.as<int32_t>();
+  seg.seg_chunk = d_seg_chunk.as<int32_t>();
+  seg.n_chunks = n_chunks;
+  seg.ng = n_seg;
+  seg.partial = d_partial.as<double>();
 
   // persistent TMA-pipelined passes for FP32 grids they support
   const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
@@ -586,8 +605,7 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
       sk.nx = g.nx;
       sk.ny = g.ny;
     }
-    MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, d_seg_idx.as<int32_t>(),
-                                 d_seg_start.as<int32_t>(), n_seg, amp_out, int_out, sk,
+    MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, seg, amp_out, int_out, sk,
                                  ctx->stream));
     if (pix_modes)
       MSF_CUDA(launch_pixel_accum(fp64, psi.p, plane, nb, plane, d_acc_a.as<double>(),
@@ -691,8 +709,9 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   {
     const int64_t n_batches = (n_probes + B - 1) / B;
     // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:
-    // 2*S slice passes, the segment sums and (pixel modes) the accumulation
-    res->kernel_launches = setup_launches + n_batches * (2 * S + 1 + (pix_modes ? 1 : 0));
+    // 2*S slice passes, the segment sums (chunks, totals) and (pixel modes)
+    // the accumulation
+    res->kernel_launches = setup_launches + n_batches * (2 * S + 2 + (pix_modes ? 1 : 0));
     ctx->d2h_bytes += (int64_t)(8 + 2 * amp.size() * sizeof(double)) +
                       (pix_modes ? 16 * plane : 0) +
                       (res->final_psi ? (int64_t)cbytes * plane : 0);

@@ -456,24 +456,8 @@ __device__ __forceinline__ double2 exit_value(const Cx<Real>* __restrict__ p, in
   return make_double2(x, y);
 }
 
-template <typename Real>
-__global__ void segment_sums_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
-                                    const int32_t* __restrict__ idx,
-                                    const int32_t* __restrict__ start, int ng,
-                                    double* amp, double* inten, const SplitK sk) {
-  __shared__ double ra[32], ri[32];
-  const int g = blockIdx.x, b = blockIdx.y;
-  const Cx<Real>* p = psi + (int64_t)b * stride;
-  const int sx = sk.psi0k ? sk.shifts[2 * b] : 0, sy = sk.psi0k ? sk.shifts[2 * b + 1] : 0;
-  double sa = 0.0, si = 0.0;
-  const int s0 = start[g], s1 = start[g + 1];
-  for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
-    const double2 v = exit_value<Real>(p, idx[k], sk, sx, sy);
-    const double x = v.x, y = v.y;
-    const double i2 = x * x + y * y;
-    si += i2;
-    sa += sqrt(i2);
-  }
+// Sum of a block's values into lane 0 of warp 0 (fixed order).
+__device__ __forceinline__ void block_sum2(double& sa, double& si, double* ra, double* ri) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     sa += __shfl_down_sync(0xffffffffu, sa, o);
@@ -491,10 +475,48 @@ __global__ void segment_sums_kernel(const Cx<Real>* __restrict__ psi, int64_t st
       sa += __shfl_down_sync(0xffffffffu, sa, o);
       si += __shfl_down_sync(0xffffffffu, si, o);
     }
-    if (l == 0) {
-      if (amp) amp[(int64_t)b * ng + g] = sa;
-      if (inten) inten[(int64_t)b * ng + g] = si;
+  }
+}
+
+// One chunk of one probe's segment pixels: partial_a/i[b * n_chunks + c].
+template <typename Real>
+__global__ void __launch_bounds__(256)
+segment_chunk_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
+                     const int32_t* __restrict__ idx, const int32_t* __restrict__ chunk_begin,
+                     int n_chunks, double* partial_a, double* partial_i, const SplitK sk) {
+  __shared__ double ra[32], ri[32];
+  const int c = blockIdx.x, b = blockIdx.y;
+  const Cx<Real>* p = psi + (int64_t)b * stride;
+  const int sx = sk.psi0k ? sk.shifts[2 * b] : 0, sy = sk.psi0k ? sk.shifts[2 * b + 1] : 0;
+  double sa = 0.0, si = 0.0;
+  const int s0 = chunk_begin[c], s1 = chunk_begin[c + 1];
+  for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
+    const double2 v = exit_value<Real>(p, __ldg(idx + k), sk, sx, sy);
+    const double i2 = v.x * v.x + v.y * v.y;
+    si += i2;
+    sa += sqrt(i2);
+  }
+  block_sum2(sa, si, ra, ri);
+  if (threadIdx.x == 0) {
+    partial_a[(int64_t)b * n_chunks + c] = sa;
+    partial_i[(int64_t)b * n_chunks + c] = si;
+  }
+}
+
+// Segment totals from the chunk sums, in chunk order: one CTA per probe.
+__global__ void segment_reduce_kernel(const double* __restrict__ partial_a,
+                                      const double* __restrict__ partial_i,
+                                      const int32_t* __restrict__ seg_chunk, int ng,
+                                      int n_chunks, double* amp, double* inten) {
+  const int b = blockIdx.x;
+  for (int g = threadIdx.x; g < ng; g += blockDim.x) {
+    double sa = 0.0, si = 0.0;
+    for (int c = seg_chunk[g]; c < seg_chunk[g + 1]; ++c) {
+      sa += partial_a[(int64_t)b * n_chunks + c];
+      si += partial_i[(int64_t)b * n_chunks + c];
     }
+    if (amp) amp[(int64_t)b * ng + g] = sa;
+    if (inten) inten[(int64_t)b * ng + g] = si;
   }
 }
 
@@ -635,16 +657,25 @@ cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t 
 }
 
 cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t stride, int nb,
-                                const int32_t* idx, const int32_t* start, int ng,
-                                double* amp, double* inten, const SplitK& sk, cudaStream_t s) {
-  if (ng <= 0 || nb <= 0) return cudaSuccess;
-  dim3 grid(ng, nb);
-  if (fp64)
-    segment_sums_kernel<double><<<grid, 256, 0, s>>>(
-        static_cast<const double2*>(psi), stride, idx, start, ng, amp, inten, sk);
-  else
-    segment_sums_kernel<float><<<grid, 256, 0, s>>>(
-        static_cast<const float2*>(psi), stride, idx, start, ng, amp, inten, sk);
+                                const SegmentPlan& sp, double* amp, double* inten,
+                                const SplitK& sk, cudaStream_t s) {
+  if (sp.ng <= 0 || nb <= 0) return cudaSuccess;
+  double* pa = sp.partial;
+  double* pi = sp.partial + (int64_t)nb * sp.n_chunks;
+  if (sp.n_chunks > 0) {
+    dim3 grid(sp.n_chunks, nb);
+    if (fp64)
+      segment_chunk_kernel<double><<<grid, 256, 0, s>>>(
+          static_cast<const double2*>(psi), stride, sp.idx, sp.chunk_begin, sp.n_chunks, pa, pi,
+          sk);
+    else
+      segment_chunk_kernel<float><<<grid, 256, 0, s>>>(
+          static_cast<const float2*>(psi), stride, sp.idx, sp.chunk_begin, sp.n_chunks, pa, pi,
+          sk);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  segment_reduce_kernel<<<nb, 128, 0, s>>>(pa, pi, sp.seg_chunk, sp.ng, sp.n_chunks, amp, inten);
   return cudaGetLastError();
 }
 

@@ -110,12 +110,22 @@ cudaError_t launch_to_f32(const double* in, float* out, int64_t n_real,
                           cudaStream_t s);
 
 // ---- detection / FEM reductions on a batch of k-space waves ----
+// Pixel segments (FEM ring bins, then the ADF annulus), each cut into chunks
+// of at most kSegmentChunk pixels so that a large segment is summed by many
+// CTAs; the chunk sums are then added in chunk order (deterministic).
+constexpr int kSegmentChunk = 2048;
+struct SegmentPlan {
+  const int32_t* idx = nullptr;          // pixel lists of all segments, concatenated
+  const int32_t* chunk_begin = nullptr;  // [n_chunks + 1] offsets into idx
+  const int32_t* seg_chunk = nullptr;    // [ng + 1] first chunk of each segment
+  int n_chunks = 0, ng = 0;
+  double* partial = nullptr;             // scratch, 2 * nb * n_chunks doubles
+};
 // For every (probe b, segment g): amp[b*ng+g] = sum |psi|, inten[...] =
-// sum |psi|^2 over pixel list idx[start[g] .. start[g+1]), FP64.
+// sum |psi|^2 over the segment's pixels, FP64 (two launches).
 cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t batch_stride,
-                                int nb, const int32_t* idx, const int32_t* start,
-                                int ng, double* amp, double* inten, const SplitK& sk,
-                                cudaStream_t s);
+                                int nb, const SegmentPlan& sp, double* amp, double* inten,
+                                const SplitK& sk, cudaStream_t s);
 // acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
                                int nb, int64_t npix, double* acc_a, double* acc_i,

@@ -179,8 +179,11 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
 }
 
 // ----------------------------------------------------- column slice pass --
+constexpr int ctas_per_256(int threads) { return threads >= 256 ? 1 : 256 / threads; }
+
 template <int N, int COLS, bool LAST>
-__global__ void __launch_bounds__(COLS * Shape<N, float>::T, 1)
+__global__ void __launch_bounds__(COLS * Shape<N, float>::T,
+                                  ctas_per_256(COLS * Shape<N, float>::T))
 col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap, int* err) {
   using C = float2;
   using Sh = Shape<N, float>;
@@ -277,10 +280,15 @@ int sm_count() {
 
 template <int N>
 constexpr int pipe_lines() { return 256 / Shape<N, float>::T; }
+// Threads per CTA of the pipelined column pass; the grid holds as many
+// persistent CTAs as fit on the SMs.
+#ifndef MSF_COL_PIPE_THREADS
+#define MSF_COL_PIPE_THREADS 256
+#endif
 template <int N>
 constexpr int pipe_cols() {
   int c = 16;
-  while (c > 1 && c * Shape<N, float>::T > 256) c >>= 1;
+  while (c > 2 && c * Shape<N, float>::T > MSF_COL_PIPE_THREADS) c >>= 1;
   return c;
 }
 
@@ -309,15 +317,17 @@ cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
   using SM = Smem<Shape<N, float>, 8, CC, true>;
   constexpr int RAW = (N * CC > CC * SM::stride ? N * CC : CC * SM::stride);
   constexpr int smem = 2 * ((RAW + 15) / 16 * 16) * 8;
-  static bool configured = false;
+  static int per_sm = 0;
   auto k = col_slice_pipe_kernel<N, CC, LAST>;
-  if (!configured) {
+  if (!per_sm) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    configured = true;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, CC * Shape<N, float>::T, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
   }
   const int items = a.nb * (a.ny / CC);
-  const int grid = items < sm_count() ? items : sm_count();
+  const int grid = items < per_sm * sm_count() ? items : per_sm * sm_count();
   k<<<grid, CC * Shape<N, float>::T, smem, s>>>(a, map, err);
   return cudaGetLastError();
 }
