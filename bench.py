@@ -75,6 +75,36 @@ def ncu_traffic(which, name="row_col_pass_1024_fp32.md"):
     return None
 
 
+def plain_and_precision(msf, job, q, z, device, argv_sample, res32):
+    """The two comparisons the headline metric is quoted with.
+
+    plain: probe*slices/s of the plain GPU path - FP64 wavefields, one probe
+    per launch, no CUDA graph, same specimen - on an 8x8 raster sample.
+    v_err: per FEM mode, the largest relative deviation over the k bins of
+    the FP32 run's V(k) from an FP64 GPU run of the full workload (bins with
+    |V| <= 1e-6 excluded)."""
+    jp = msf.Job(argv_sample)
+    cp = msf.Context(device=device, precision="fp64", batch=1, graphs=False)
+    sp = cp.specimen(jp.grid, q, z)
+    cp.run(sp, jp.optics, jp.raster, jp.detect)
+    rp = cp.run(sp, jp.optics, jp.raster, jp.detect)
+    plain = rp.probe_slices / rp.seconds_raster
+    sp.close()
+    cp.close()
+    c64 = msf.Context(device=device, precision="fp64")
+    s64 = c64.specimen(job.grid, q, z)
+    r64 = c64.run(s64, job.optics, job.raster, job.detect)
+    errs = {}
+    for m, v64 in r64.v.items():
+        v32 = res32.v[m]
+        ok = np.isfinite(v64) & (np.abs(v64) > 1e-6)
+        errs[m] = float(np.max(np.abs(v32[ok] - v64[ok]) / np.abs(v64[ok]))) if ok.any() else None
+    fp64_rate = r64.probe_slices / r64.seconds_raster
+    s64.close()
+    c64.close()
+    return plain, errs, fp64_rate
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
 
@@ -213,6 +243,8 @@ def main():
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain-path and FP64 comparison runs")
     ap.add_argument("--raster", type=int, default=0,
                     help="probes per raster side (default 64, the workload's); smaller "
                          "values make a short case for profiling")
@@ -259,6 +291,7 @@ def main():
         wall0 = time.time()
         for _ in range(args.steps):
             r = ctx.run(spec, job.optics, job.raster, job.detect)
+            last = r
             dev_times.append(r.seconds_raster)
             launches += r.kernel_launches
             ps += r.probe_slices
@@ -317,6 +350,19 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e["value"] = e2e_ps * world / float(t.item())
 
+    # plain one-probe-at-a-time GPU path and the FP32 outputs' error
+    versus = None
+    if world == 1 and not args.no_plain and args.precision == "fp32":
+        sample = list(argv)
+        sample[sample.index("--rasterspacing") + 1] = repr(WORKLOAD["box"][0] / 8)
+        plain, v_err, fp64_rate = plain_and_precision(msf, job, q, z, local, sample, last)
+        versus = {"plain_gpu": {"value": round(plain, 1), "unit": UNIT,
+                                "path": "FP64 wavefields, 1 probe per launch, no CUDA graph",
+                                "sample": "8x8 raster of the same specimen"},
+                  "batched_vs_plain": round(value / plain, 2),
+                  "fp64_batched": {"value": round(fp64_rate, 1), "unit": UNIT},
+                  "v_err_vs_fp64": v_err, "v_err_bound": 1e-4}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         s = reference_sample(os.cpu_count() or 1)
@@ -338,7 +384,7 @@ def main():
                                  (spec.device_bytes() / 1e6),
                            "graphs": not args.no_graphs, "batch": args.batch or "auto",
                            "specimen_setup_s": round(setup_s, 3)},
-                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "versus": versus,
                 "clocks": clocks.summary(), "gpu_launches": int(launches),
                 "wall_s_timed": round(wall, 3)}
         print(json.dumps(line))

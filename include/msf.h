@@ -184,6 +184,59 @@ msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
 msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
                              double* probe_device, void* stream);
 
+/* ---- slot batches and serving (no counterpart in the reference) -------- */
+/* Several rasters at once: results[i] is what msf_run(ctx, specs[i],
+ * &optics[i], &rasters[i], &detects[i], &results[i]) returns, within FP32
+ * rounding (final_psi is not filled).  Rasters of the same grid size share
+ * launches: each of `slots` wavefields (0: up to 256, bounded by free
+ * memory) carries one probe of any raster at its own slice, and a slot whose
+ * probe finished is refilled with the next waiting probe.  Grid sizes run as
+ * separate lanes on separate streams that overlap on the GPU.  FP32 contexts
+ * only.  results[i].seconds_raster is the device time from the start of the
+ * batch to the completion of raster i; kernel_launches counts the launches
+ * of its lane. */
+msf_status msf_run_batch(msf_context* ctx, int32_t n, const msf_specimen* const* specs,
+                         const msf_optics* optics, const msf_raster* rasters,
+                         const msf_detect* detects, msf_results* results,
+                         int32_t slots);
+
+/* A simulation request: everything is copied at submission. */
+typedef struct {
+  msf_grid grid;
+  msf_atoms atoms;
+  msf_optics optics;
+  msf_raster raster;
+  msf_detect detect;
+} msf_request;
+
+typedef struct {
+  int64_t submitted, completed, failed, running, waiting;
+  double p50_s, p99_s, max_s;  /* latency, submission to completion         */
+  double probe_slices_per_s;   /* completed probe*slices / busy wall time    */
+  int64_t probe_slices;
+  int64_t device_bytes;        /* bytes the server holds now                */
+} msf_server_stats;
+
+typedef struct msf_server msf_server;
+/* A request loop on one GPU (FP32 wavefields).  A worker thread admits
+ * requests in arrival order while their estimated device bytes fit
+ * `opt->hbm_budget` (0: 80 % of free memory), builds each specimen, and
+ * feeds its probes into the slot lane of its grid size (`slots` wavefields
+ * per lane, 0: 64); requests that arrive while others run join the running
+ * launches as slots free up. */
+msf_status msf_server_create(const msf_options* opt, int32_t slots, msf_server** out);
+/* Queue a request; returns at once with its ticket. */
+msf_status msf_server_submit(msf_server* srv, const msf_request* req, uint64_t* ticket);
+/* MSF_OK and the results (as msf_run fills them) when the request finished,
+ * MSF_ERR_BUSY while it is queued or running after waiting up to wait_ms,
+ * or the request's error status.  A finished request is forgotten after its
+ * first successful poll. */
+msf_status msf_server_poll(msf_server* srv, uint64_t ticket, int32_t wait_ms,
+                           msf_results* results);
+msf_status msf_server_stats_get(msf_server* srv, msf_server_stats* out);
+/* Finishes the running and queued requests, then stops the worker. */
+msf_status msf_server_destroy(msf_server* srv);
+
 /* ---- host-side set-up helpers (bit-exact with the reference) ----------- */
 /* lambda [A] and gamma for an accelerating voltage (tem.cpp:424-438). */
 void msf_wavelength(double voltage, double* lambda, double* gamma);

@@ -192,6 +192,13 @@ msf_status msf_run(msf_context* ctx, const msf_specimen* spec, const msf_optics*
   return run_raster(ctx, spec, optics, raster, detect, results);
 }
 
+msf_status msf_run_batch(msf_context* ctx, int32_t n, const msf_specimen* const* specs,
+                         const msf_optics* optics, const msf_raster* rasters,
+                         const msf_detect* detects, msf_results* results, int32_t slots) {
+  if (!ctx) return MSF_ERR_ARG;
+  return run_batch(ctx, n, specs, optics, rasters, detects, results, slots);
+}
+
 msf_status msf_probe(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                      double* out) {
   if (!ctx || !spec || !optics || !out) return MSF_ERR_ARG;

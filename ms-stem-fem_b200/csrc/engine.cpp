@@ -412,45 +412,60 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   return MSF_OK;
 }
 
-msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
-                      const msf_raster* raster, const msf_detect* det, msf_results* res) {
-  if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
+int64_t raster_plan_bytes(const msf_specimen* spec, bool fp64, int64_t n_probes,
+                          bool pix_modes) {
+  const int64_t plane = (int64_t)spec->g.nx * spec->g.ny;
+  int64_t b = 16 * plane;                                    // probe
+  if (!fp64) b += 8 * plane * spec->n_slices + 16 * plane;   // vacuum tables
+  b += 8 * n_probes + 3 * 4 * plane;                         // shifts, segments
+  b += 2 * 8 * n_probes * (int64_t)(spec->g.nx + 1);         // sums (n_seg <= nx + 1)
+  if (pix_modes) b += 2 * 8 * plane;
+  return b;
+}
+
+msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                       const msf_raster* raster, const msf_detect* det, RasterPlan* P) {
+  if (!spec || !optics || !raster || !det || !P) { set_error("null argument"); return MSF_ERR_ARG; }
   const Grid& g = spec->g;
   const int64_t plane = (int64_t)g.nx * g.ny;
   const bool fp64 = ctx->fp64;
-  const size_t cbytes = fp64 ? 16 : 8;
   const int S = spec->n_slices;
+  if (S <= 0) { set_error("specimen has no slices"); return MSF_ERR_ARG; }
   std::vector<double> x_p(raster->x_p, raster->x_p + std::max(0, raster->n_x));
   std::vector<double> y_p(raster->y_p, raster->y_p + std::max(0, raster->n_y));
   const int64_t n_probes = (int64_t)x_p.size() * (int64_t)y_p.size();
   if (n_probes <= 0) { set_error("empty raster"); return MSF_ERR_ARG; }
-  const bool want_adf = det->outputs & MSF_OUT_ADF_IMAGE;
-  const uint32_t fem = det->outputs & MSF_OUT_FEM_MASK;
-  const bool pix_modes = det->outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE |
-                                         MSF_OUT_V_GT17 | MSF_OUT_V_RBAR);
+  P->spec = spec;
+  P->optics = *optics;
+  P->det = *det;
+  P->n_probes = n_probes;
+  P->S = S;
+  P->plane = plane;
+  P->want_adf = det->outputs & MSF_OUT_ADF_IMAGE;
+  P->fem = det->outputs & MSF_OUT_FEM_MASK;
+  P->pix_modes = det->outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE | MSF_OUT_V_GT17 |
+                                 MSF_OUT_V_RBAR);
   MSF_CUDA(cudaSetDevice(ctx->device));
 
   // probe
-  DevBuf probe64;
-  MSF_TRY(build_probe(ctx, spec, optics, &probe64));
-  const void* probe = probe64.p;
-  int64_t setup_launches = 5;
+  MSF_TRY(build_probe(ctx, spec, optics, &P->probe64));
+  P->setup_launches = 5;
 
   // FP32 runs carry only the scattered part of each wave; the vacuum part
   // psi0 (the probe propagated with t = 1) is the same for every probe up to
   // its integer shift, so it is built once here in FP64: psi0_tab[s] is the
   // real-space vacuum wave entering slice s (in the scale of the inverse-
   // transformed buffer) and psi0k the vacuum exit wave in k-space.
-  DevBuf psi0_tab, psi0k, prop64;
   if (!fp64) {
-    MSF_TRY(ctx->alloc(&psi0_tab, 8 * plane * (size_t)S));
-    MSF_TRY(ctx->alloc(&psi0k, 16 * plane));
+    DevBuf prop64;
+    MSF_TRY(ctx->alloc(&P->psi0_tab, 8 * plane * (size_t)S));
+    MSF_TRY(ctx->alloc(&P->psi0k, 16 * plane));
     MSF_TRY(upload(ctx, &prop64, spec->hprop));
-    MSF_CUDA(cudaMemcpyAsync(psi0k.p, probe64.p, 16 * plane, cudaMemcpyDeviceToDevice,
+    MSF_CUDA(cudaMemcpyAsync(P->psi0k.p, P->probe64.p, 16 * plane, cudaMemcpyDeviceToDevice,
                              ctx->stream));
-    MSF_CUDA(launch_scale(psi0k.as<double>(), plane, g.nxny / g.s, nullptr, ctx->stream));
+    MSF_CUDA(launch_scale(P->psi0k.as<double>(), plane, g.nxny / g.s, nullptr, ctx->stream));
     PassArgs v;
-    v.psi = psi0k.p;
+    v.psi = P->psi0k.p;
     v.batch_stride = plane;
     v.nb = 1;
     v.nx = g.nx;
@@ -461,9 +476,9 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     const void *tw_y = nullptr, *tw_x = nullptr;
     MSF_TRY(ctx->twiddles(g.ny, true, &tw_y));
     MSF_TRY(ctx->twiddles(g.nx, true, &tw_x));
-    setup_launches += 1;
+    P->setup_launches += 1;
     for (int s = 0; s < S; ++s) {
-      MSF_CUDA(launch_to_f32(psi0k.as<double>(), psi0_tab.as<float>() + 2 * plane * s,
+      MSF_CUDA(launch_to_f32(P->psi0k.as<double>(), P->psi0_tab.as<float>() + 2 * plane * s,
                              2 * plane, ctx->stream));
       v.tw = tw_y;
       MSF_CUDA(launch_row(true, ROW_FWD, v, ctx->stream));
@@ -471,265 +486,101 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
       v.px = prop64.as<double>() + 2 * (size_t)(g.nx + g.ny) * s;
       v.py = prop64.as<double>() + 2 * (size_t)(g.nx + g.ny) * s + 2 * g.nx;
       MSF_CUDA(launch_col(true, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, v, ctx->stream));
-      setup_launches += 3;
+      P->setup_launches += 3;
       if (s + 1 < S) {
         v.tw = tw_y;
         v.scale = 1.0;
         MSF_CUDA(launch_row(true, ROW_INV, v, ctx->stream));
-        setup_launches += 1;
+        P->setup_launches += 1;
       }
     }
+    // prop64 is released at the end of this scope: finish its readers first
+    MSF_CUDA(cudaStreamSynchronize(ctx->stream));
   }
 
   // per-probe pixel shifts
-  std::vector<int32_t> shifts;
-  if (!probe_shifts(g, x_p, y_p, &shifts)) {
+  if (!probe_shifts(g, x_p, y_p, &P->shifts)) {
     set_error("a raster position lies half a pixel or more below the cell origin");
     return MSF_ERR_ARG;
   }
-  DevBuf d_shifts;
-  MSF_TRY(upload(ctx, &d_shifts, shifts));
+  MSF_TRY(upload(ctx, &P->d_shifts, P->shifts));
 
   // segments: ring bins (FEM) then the ADF detector annulus
-  Rings rings;
-  if (fem) rings = make_rings(g, det->dr);
-  const int n_k = fem ? rings.n_k : 0;
+  if (P->fem) P->rings = make_rings(g, det->dr);
+  P->n_k = P->fem ? P->rings.n_k : 0;
   std::vector<int32_t> seg_idx, seg_start{0};
-  if (fem) {
-    seg_idx = rings.pix;
-    for (int k = 0; k < n_k; ++k) seg_start.push_back(rings.start[k + 1]);
+  if (P->fem) {
+    seg_idx = P->rings.pix;
+    for (int k = 0; k < P->n_k; ++k) seg_start.push_back(P->rings.start[k + 1]);
   }
   const std::vector<int32_t> adf_pix =
       detector_pixels(g, det->det_inner / g.lambda, det->det_outer / g.lambda);
   seg_idx.insert(seg_idx.end(), adf_pix.begin(), adf_pix.end());
   seg_start.push_back((int32_t)seg_idx.size());
-  const int n_seg = n_k + 1;
+  P->n_seg = P->n_k + 1;
   // chunks of at most kSegmentChunk pixels, never straddling two segments
   std::vector<int32_t> chunk_begin, seg_chunk;
-  for (int gi = 0; gi < n_seg; ++gi) {
+  for (int gi = 0; gi < P->n_seg; ++gi) {
     seg_chunk.push_back((int32_t)chunk_begin.size());
     for (int32_t k = seg_start[gi]; k < seg_start[gi + 1]; k += kSegmentChunk)
       chunk_begin.push_back(k);
   }
   seg_chunk.push_back((int32_t)chunk_begin.size());
-  const int n_chunks = (int)chunk_begin.size();
-  chunk_begin.push_back(seg_start[n_seg]);
-  DevBuf d_seg_idx, d_chunk_begin, d_seg_chunk, d_partial, d_amp, d_int, d_acc_a, d_acc_i;
-  MSF_TRY(upload(ctx, &d_seg_idx, seg_idx));
-  MSF_TRY(upload(ctx, &d_chunk_begin, chunk_begin));
-  MSF_TRY(upload(ctx, &d_seg_chunk, seg_chunk));
-  MSF_TRY(ctx->alloc(&d_amp, sizeof(double) * n_probes * n_seg));
-  MSF_TRY(ctx->alloc(&d_int, sizeof(double) * n_probes * n_seg));
-  if (pix_modes) {
-    MSF_TRY(ctx->alloc(&d_acc_a, sizeof(double) * plane));
-    MSF_TRY(ctx->alloc(&d_acc_i, sizeof(double) * plane));
-    MSF_CUDA(cudaMemsetAsync(d_acc_a.p, 0, d_acc_a.bytes, ctx->stream));
-    MSF_CUDA(cudaMemsetAsync(d_acc_i.p, 0, d_acc_i.bytes, ctx->stream));
+  P->n_chunks = (int)chunk_begin.size();
+  chunk_begin.push_back(seg_start[P->n_seg]);
+  MSF_TRY(upload(ctx, &P->seg_idx, seg_idx));
+  MSF_TRY(upload(ctx, &P->chunk_begin, chunk_begin));
+  MSF_TRY(upload(ctx, &P->seg_chunk, seg_chunk));
+  MSF_TRY(ctx->alloc(&P->amp, sizeof(double) * n_probes * P->n_seg));
+  MSF_TRY(ctx->alloc(&P->inten, sizeof(double) * n_probes * P->n_seg));
+  if (P->pix_modes) {
+    MSF_TRY(ctx->alloc(&P->acc_a, sizeof(double) * plane));
+    MSF_TRY(ctx->alloc(&P->acc_i, sizeof(double) * plane));
+    MSF_CUDA(cudaMemsetAsync(P->acc_a.p, 0, P->acc_a.bytes, ctx->stream));
+    MSF_CUDA(cudaMemsetAsync(P->acc_i.p, 0, P->acc_i.bytes, ctx->stream));
   }
+  // the host vectors above are staged by pageable copies: complete them
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MSF_OK;
+}
 
-  // batch of wavefields
-  int B = ctx->batch;
-  if (B <= 0) {
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    const int64_t cap = (int64_t)(0.5 * (double)free_b) / (int64_t)(cbytes * plane);
-    B = (int)std::max<int64_t>(1, std::min<int64_t>(cap, 64));
-  }
-  B = (int)std::min<int64_t>(B, n_probes);
-  DevBuf psi;
-  MSF_TRY(ctx->alloc(&psi, cbytes * plane * B));
-  MSF_TRY(ctx->alloc(&d_partial, sizeof(double) * 2 * B * std::max(n_chunks, 1)));
-  SegmentPlan seg;
-  seg.idx = d_seg_idx.as<int32_t>();
-  seg.chunk_begin = d_chunk_begin.as<int32_t>();
-  seg.seg_chunk = d_seg_chunk.as<int32_t>();
-  seg.n_chunks = n_chunks;
-  seg.ng = n_seg;
-  seg.partial = d_partial.as<double>();
-
-  // persistent TMA-pipelined passes for FP32 grids they support
-  const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
-  const bool pipe_row = pipe_ok && (ctx->pipe & MSF_PIPE_ROW);
-  const bool pipe_col = pipe_ok && (ctx->pipe & MSF_PIPE_COL);
-  alignas(64) unsigned char col_map[128];
-  DevBuf d_err;
-  MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
-  MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
-  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map));
-
-  PassArgs row, col;
-  row.psi = col.psi = psi.p;
-  row.batch_stride = col.batch_stride = plane;
-  row.nx = col.nx = g.nx;
-  row.ny = col.ny = g.ny;
-  MSF_TRY(ctx->twiddles(g.ny, fp64, &row.tw));
-  MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
-  row.inv_s = col.inv_s = 1.0 / g.s;
-  row.probe = probe;
-  row.first_scale = g.nxny / g.s;
-  col.mask_lo = spec->mask_lo.as<int32_t>();
-  col.mask_hi = spec->mask_hi.as<int32_t>();
-  const char* tbase = static_cast<const char*>(spec->t.p);
-  const char* pbase = static_cast<const char*>(spec->prop.p);
-  const size_t prop_stride = cbytes * (g.nx + g.ny);
-
-  // one batch: 2*S fused passes then the reductions
-  auto enqueue_batch = [&](int nb, const int32_t* shifts_dev, double* amp_out,
-                           double* int_out) -> msf_status {
-    row.nb = col.nb = nb;
-    row.shifts = shifts_dev;
-    for (int s = 0; s < S; ++s) {
-      row.trans = tbase + cbytes * plane * s;
-      RowOp op;
-      if (fp64) {
-        op = s == 0 ? ROW_SLICE_FIRST : ROW_SLICE;
-      } else {
-        op = s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT;
-        row.psi0 = psi0_tab.as<float>() + 2 * plane * s;
-      }
-      if (pipe_row && op == ROW_SPLIT)
-        MSF_CUDA(launch_row_split_pipe(row, d_err.as<int>(), ctx->stream));
-      else
-        MSF_CUDA(launch_row(fp64, op, row, ctx->stream));
-      col.px = pbase + prop_stride * s;
-      col.py = pbase + prop_stride * s + cbytes * g.nx;
-      if (pipe_col)
-        MSF_CUDA(launch_col_slice_pipe(col, s + 1 == S, col_map, d_err.as<int>(), ctx->stream));
-      else
-        MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
-    }
-    SplitK sk;
-    if (!fp64) {
-      sk.psi0k = psi0k.as<double>();
-      sk.shifts = shifts_dev;
-      sk.nx = g.nx;
-      sk.ny = g.ny;
-    }
-    MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, seg, amp_out, int_out, sk,
-                                 ctx->stream));
-    if (pix_modes)
-      MSF_CUDA(launch_pixel_accum(fp64, psi.p, plane, nb, plane, d_acc_a.as<double>(),
-                                  d_acc_i.as<double>(), sk, ctx->stream));
-    return MSF_OK;
-  };
-  if (S <= 0) { set_error("specimen has no slices"); return MSF_ERR_ARG; }
-
-  cudaEvent_t ev0, ev1;
-  MSF_CUDA(cudaEventCreate(&ev0));
-  MSF_CUDA(cudaEventCreate(&ev1));
-  MSF_CUDA(cudaEventRecord(ev0, ctx->stream));
-  cudaGraphExec_t graph_exec = nullptr;
-  DevBuf stage_shift, stage_amp, stage_int;
-  const bool use_graph = ctx->graphs && n_probes / B >= 2;
-  if (use_graph) {
-    MSF_TRY(ctx->alloc(&stage_shift, sizeof(int32_t) * 2 * B));
-    MSF_TRY(ctx->alloc(&stage_amp, sizeof(double) * B * n_seg));
-    MSF_TRY(ctx->alloc(&stage_int, sizeof(double) * B * n_seg));
-  }
-  msf_status st = MSF_OK;
-  for (int64_t p0 = 0; p0 < n_probes && st == MSF_OK; p0 += B) {
-    const int nb = (int)std::min<int64_t>(B, n_probes - p0);
-    if (use_graph && nb == B && p0 > 0) {
-      MSF_CUDA(cudaMemcpyAsync(stage_shift.p, d_shifts.as<int32_t>() + 2 * p0,
-                               sizeof(int32_t) * 2 * nb, cudaMemcpyDeviceToDevice, ctx->stream));
-      if (!graph_exec) {
-        cudaGraph_t graph;
-        MSF_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        st = enqueue_batch(nb, stage_shift.as<int32_t>(), stage_amp.as<double>(),
-                           stage_int.as<double>());
-        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
-        if (st != MSF_OK) break;
-        MSF_CUDA(ce);
-        MSF_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
-        cudaGraphDestroy(graph);
-      }
-      MSF_CUDA(cudaGraphLaunch(graph_exec, ctx->stream));
-      MSF_CUDA(cudaMemcpyAsync(d_amp.as<double>() + p0 * n_seg, stage_amp.p,
-                               sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
-                               ctx->stream));
-      MSF_CUDA(cudaMemcpyAsync(d_int.as<double>() + p0 * n_seg, stage_int.p,
-                               sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
-                               ctx->stream));
-    } else {
-      st = enqueue_batch(nb, d_shifts.as<int32_t>() + 2 * p0, d_amp.as<double>() + p0 * n_seg,
-                         d_int.as<double>() + p0 * n_seg);
-    }
-  }
-  if (graph_exec) cudaGraphExecDestroy(graph_exec);
-  if (st != MSF_OK) return st;
-  MSF_CUDA(cudaEventRecord(ev1, ctx->stream));
-
-  // copy back
+msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t stream,
+                         msf_results* res) {
+  const Grid& g = P.spec->g;
+  const int64_t plane = P.plane, n_probes = P.n_probes;
+  const int n_k = P.n_k, n_seg = P.n_seg;
   std::vector<double> amp((size_t)n_probes * n_seg), inten((size_t)n_probes * n_seg);
-  MSF_CUDA(cudaMemcpyAsync(amp.data(), d_amp.p, amp.size() * sizeof(double),
-                           cudaMemcpyDeviceToHost, ctx->stream));
-  MSF_CUDA(cudaMemcpyAsync(inten.data(), d_int.p, inten.size() * sizeof(double),
-                           cudaMemcpyDeviceToHost, ctx->stream));
+  MSF_CUDA(cudaMemcpyAsync(amp.data(), P.amp.p, amp.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, stream));
+  MSF_CUDA(cudaMemcpyAsync(inten.data(), P.inten.p, inten.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, stream));
   std::vector<double> acc_a, acc_i;
-  if (pix_modes) {
+  if (P.pix_modes) {
     acc_a.resize(plane);
     acc_i.resize(plane);
-    MSF_CUDA(cudaMemcpyAsync(acc_a.data(), d_acc_a.p, plane * sizeof(double),
-                             cudaMemcpyDeviceToHost, ctx->stream));
-    MSF_CUDA(cudaMemcpyAsync(acc_i.data(), d_acc_i.p, plane * sizeof(double),
-                             cudaMemcpyDeviceToHost, ctx->stream));
+    MSF_CUDA(cudaMemcpyAsync(acc_a.data(), P.acc_a.p, plane * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream));
+    MSF_CUDA(cudaMemcpyAsync(acc_i.data(), P.acc_i.p, plane * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream));
   }
-  if (res->final_psi) {
-    const int last = (int)((n_probes - 1) % B);
-    if (fp64) {
-      MSF_CUDA(cudaMemcpyAsync(res->final_psi, psi.as<double>() + 2 * plane * last,
-                               16 * plane, cudaMemcpyDeviceToHost, ctx->stream));
-    } else {
-      // exit wave = scattered part + the vacuum part at this probe's shift
-      DevBuf full;
-      MSF_TRY(ctx->alloc(&full, 16 * plane));
-      const int64_t pl = n_probes - 1;
-      MSF_CUDA(launch_assemble_split(psi.as<float>() + 2 * plane * last, psi0k.as<double>(),
-                                     g.nx, g.ny, shifts[2 * pl], shifts[2 * pl + 1],
-                                     full.as<double>(), ctx->stream));
-      MSF_CUDA(cudaMemcpyAsync(res->final_psi, full.p, 16 * plane, cudaMemcpyDeviceToHost,
-                               ctx->stream));
-      MSF_CUDA(cudaStreamSynchronize(ctx->stream));
-    }
-  }
-  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
-  int err_flag = 0;
-  MSF_CUDA(cudaMemcpy(&err_flag, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err_flag) {
-    set_error("a pipelined slice pass gave up waiting for a tile copy (bounded wait)");
-    return MSF_ERR_TIMEOUT;
-  }
-  float ms = 0;
-  MSF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
-  res->seconds_raster = 1e-3 * ms;
-  res->seconds_setup = 0;
-  res->probe_slices = n_probes * S;
-  {
-    const int64_t n_batches = (n_probes + B - 1) / B;
-    // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:
-    // 2*S slice passes, the segment sums (chunks, totals) and (pixel modes)
-    // the accumulation
-    res->kernel_launches = setup_launches + n_batches * (2 * S + 2 + (pix_modes ? 1 : 0));
-    ctx->d2h_bytes += (int64_t)(8 + 2 * amp.size() * sizeof(double)) +
-                      (pix_modes ? 16 * plane : 0) +
-                      (res->final_psi ? (int64_t)cbytes * plane : 0);
-  }
+  MSF_CUDA(cudaStreamSynchronize(stream));
+  ctx->d2h_bytes += (int64_t)(2 * amp.size() * sizeof(double)) + (P.pix_modes ? 16 * plane : 0);
 
-  if (want_adf && res->adf_image)
+  if (P.want_adf && res->adf_image)
     for (int64_t p = 0; p < n_probes; ++p) res->adf_image[p] = inten[p * n_seg + n_k];
 
   // ---- FEM statistics on the host, in the reference's order -----------
   res->n_k = n_k;
-  if (!fem) return MSF_OK;
+  if (!P.fem) return MSF_OK;
   if (n_k > res->cap_k) {
     set_error("results.cap_k is smaller than the number of k bins (" + std::to_string(n_k) + ")");
     return MSF_ERR_ARG;
   }
+  const Rings& rings = P.rings;
+  const msf_detect* det = &P.det;
   std::vector<uint8_t> inside(n_k);
   for (int k = 0; k < n_k; ++k)
-    inside[k] = (g.lambda * rings.bounds[k + 1] <= optics->alpha_max);  // adfstem.cpp:2518
+    inside[k] = (g.lambda * rings.bounds[k + 1] <= P.optics.alpha_max);  // adfstem.cpp:2518
   const std::vector<int32_t>& cnt = rings.counts;
   for (int k = 0; k < n_k; ++k) {
     if (res->k_lower) res->k_lower[k] = rings.bounds[k];
@@ -760,7 +611,7 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
       if (res->vbar_r && (det->outputs & MSF_OUT_VBAR_R)) res->vbar_r[k] = vs[k] / n_r;
     }
   }
-  if (pix_modes) {  // adfstem.cpp:2926-3612
+  if (P.pix_modes) {  // adfstem.cpp:2926-3612
     std::vector<double> mean_a(plane), mean_sq(plane), mean_i(plane), var(plane);
     for (int64_t p = 0; p < plane; ++p) {
       mean_a[p] = acc_a[p] / n_r;
@@ -791,7 +642,8 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
         res->v_rbar[k] = ((r2[k] / c) / (r3[k] * r3[k] / cc)) - 1.0;
     }
     if (res->omega_vimage && (det->outputs & MSF_OUT_OMEGA_VIMAGE)) {
-      const double lsq = g.lambda * g.lambda, amax_sq = optics->alpha_max * optics->alpha_max;
+      const double lsq = g.lambda * g.lambda;
+      const double amax_sq = P.optics.alpha_max * P.optics.alpha_max;
       for (int i = 0; i < g.nx; ++i)
         for (int j = 0; j < g.ny; ++j) {
           const int64_t p = j + (int64_t)g.ny * i;
@@ -805,6 +657,193 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     }
   }
   return MSF_OK;
+}
+
+msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                      const msf_raster* raster, const msf_detect* det, msf_results* res) {
+  if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
+  RasterPlan P;
+  MSF_TRY(plan_raster(ctx, spec, optics, raster, det, &P));
+  const Grid& g = spec->g;
+  const int64_t plane = P.plane, n_probes = P.n_probes;
+  const bool fp64 = ctx->fp64;
+  const size_t cbytes = fp64 ? 16 : 8;
+  const int S = P.S, n_seg = P.n_seg;
+
+  // batch of wavefields
+  int B = ctx->batch;
+  if (B <= 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const int64_t cap = (int64_t)(0.5 * (double)free_b) / (int64_t)(cbytes * plane);
+    B = (int)std::max<int64_t>(1, std::min<int64_t>(cap, 64));
+  }
+  B = (int)std::min<int64_t>(B, n_probes);
+  DevBuf psi, d_partial;
+  MSF_TRY(ctx->alloc(&psi, cbytes * plane * B));
+  MSF_TRY(ctx->alloc(&d_partial, sizeof(double) * 2 * B * std::max(P.n_chunks, 1)));
+  SegmentPlan seg;
+  seg.idx = P.seg_idx.as<int32_t>();
+  seg.chunk_begin = P.chunk_begin.as<int32_t>();
+  seg.seg_chunk = P.seg_chunk.as<int32_t>();
+  seg.n_chunks = P.n_chunks;
+  seg.ng = n_seg;
+  seg.partial = d_partial.as<double>();
+
+  // persistent TMA-pipelined passes for FP32 grids they support
+  const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
+  const bool pipe_row = pipe_ok && (ctx->pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_ok && (ctx->pipe & MSF_PIPE_COL);
+  alignas(64) unsigned char col_map[128];
+  DevBuf d_err;
+  MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
+  MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
+  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map));
+
+  PassArgs row, col;
+  row.psi = col.psi = psi.p;
+  row.batch_stride = col.batch_stride = plane;
+  row.nx = col.nx = g.nx;
+  row.ny = col.ny = g.ny;
+  MSF_TRY(ctx->twiddles(g.ny, fp64, &row.tw));
+  MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
+  row.inv_s = col.inv_s = 1.0 / g.s;
+  row.probe = P.probe64.p;
+  row.first_scale = g.nxny / g.s;
+  col.mask_lo = spec->mask_lo.as<int32_t>();
+  col.mask_hi = spec->mask_hi.as<int32_t>();
+  const char* tbase = static_cast<const char*>(spec->t.p);
+  const char* pbase = static_cast<const char*>(spec->prop.p);
+  const size_t prop_stride = cbytes * (g.nx + g.ny);
+
+  // one batch: 2*S fused passes then the reductions
+  auto enqueue_batch = [&](int nb, const int32_t* shifts_dev, double* amp_out,
+                           double* int_out) -> msf_status {
+    row.nb = col.nb = nb;
+    row.shifts = shifts_dev;
+    for (int s = 0; s < S; ++s) {
+      row.trans = tbase + cbytes * plane * s;
+      RowOp op;
+      if (fp64) {
+        op = s == 0 ? ROW_SLICE_FIRST : ROW_SLICE;
+      } else {
+        op = s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT;
+        row.psi0 = P.psi0_tab.as<float>() + 2 * plane * s;
+      }
+      if (pipe_row && op == ROW_SPLIT)
+        MSF_CUDA(launch_row_split_pipe(row, d_err.as<int>(), ctx->stream));
+      else
+        MSF_CUDA(launch_row(fp64, op, row, ctx->stream));
+      col.px = pbase + prop_stride * s;
+      col.py = pbase + prop_stride * s + cbytes * g.nx;
+      if (pipe_col)
+        MSF_CUDA(launch_col_slice_pipe(col, s + 1 == S, col_map, d_err.as<int>(), ctx->stream));
+      else
+        MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
+    }
+    SplitK sk;
+    if (!fp64) {
+      sk.psi0k = P.psi0k.as<double>();
+      sk.shifts = shifts_dev;
+      sk.nx = g.nx;
+      sk.ny = g.ny;
+    }
+    MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, seg, amp_out, int_out, sk,
+                                 ctx->stream));
+    if (P.pix_modes)
+      MSF_CUDA(launch_pixel_accum(fp64, psi.p, plane, nb, plane, P.acc_a.as<double>(),
+                                  P.acc_i.as<double>(), sk, ctx->stream));
+    return MSF_OK;
+  };
+
+  cudaEvent_t ev0, ev1;
+  MSF_CUDA(cudaEventCreate(&ev0));
+  MSF_CUDA(cudaEventCreate(&ev1));
+  MSF_CUDA(cudaEventRecord(ev0, ctx->stream));
+  cudaGraphExec_t graph_exec = nullptr;
+  DevBuf stage_shift, stage_amp, stage_int;
+  const bool use_graph = ctx->graphs && n_probes / B >= 2;
+  if (use_graph) {
+    MSF_TRY(ctx->alloc(&stage_shift, sizeof(int32_t) * 2 * B));
+    MSF_TRY(ctx->alloc(&stage_amp, sizeof(double) * B * n_seg));
+    MSF_TRY(ctx->alloc(&stage_int, sizeof(double) * B * n_seg));
+  }
+  msf_status st = MSF_OK;
+  for (int64_t p0 = 0; p0 < n_probes && st == MSF_OK; p0 += B) {
+    const int nb = (int)std::min<int64_t>(B, n_probes - p0);
+    if (use_graph && nb == B && p0 > 0) {
+      MSF_CUDA(cudaMemcpyAsync(stage_shift.p, P.d_shifts.as<int32_t>() + 2 * p0,
+                               sizeof(int32_t) * 2 * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (!graph_exec) {
+        cudaGraph_t graph;
+        MSF_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_batch(nb, stage_shift.as<int32_t>(), stage_amp.as<double>(),
+                           stage_int.as<double>());
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (st != MSF_OK) break;
+        MSF_CUDA(ce);
+        MSF_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+        cudaGraphDestroy(graph);
+      }
+      MSF_CUDA(cudaGraphLaunch(graph_exec, ctx->stream));
+      MSF_CUDA(cudaMemcpyAsync(P.amp.as<double>() + p0 * n_seg, stage_amp.p,
+                               sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+      MSF_CUDA(cudaMemcpyAsync(P.inten.as<double>() + p0 * n_seg, stage_int.p,
+                               sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    } else {
+      st = enqueue_batch(nb, P.d_shifts.as<int32_t>() + 2 * p0, P.amp.as<double>() + p0 * n_seg,
+                         P.inten.as<double>() + p0 * n_seg);
+    }
+  }
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (st != MSF_OK) return st;
+  MSF_CUDA(cudaEventRecord(ev1, ctx->stream));
+
+  if (res->final_psi) {
+    const int last = (int)((n_probes - 1) % B);
+    if (fp64) {
+      MSF_CUDA(cudaMemcpyAsync(res->final_psi, psi.as<double>() + 2 * plane * last,
+                               16 * plane, cudaMemcpyDeviceToHost, ctx->stream));
+    } else {
+      // exit wave = scattered part + the vacuum part at this probe's shift
+      DevBuf full;
+      MSF_TRY(ctx->alloc(&full, 16 * plane));
+      const int64_t pl = n_probes - 1;
+      MSF_CUDA(launch_assemble_split(psi.as<float>() + 2 * plane * last, P.psi0k.as<double>(),
+                                     g.nx, g.ny, P.shifts[2 * pl], P.shifts[2 * pl + 1],
+                                     full.as<double>(), ctx->stream));
+      MSF_CUDA(cudaMemcpyAsync(res->final_psi, full.p, 16 * plane, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+      MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->d2h_bytes += (int64_t)cbytes * plane;
+  }
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  int err_flag = 0;
+  MSF_CUDA(cudaMemcpy(&err_flag, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  ctx->d2h_bytes += 8;
+  if (err_flag) {
+    set_error("a pipelined slice pass gave up waiting for a tile copy (bounded wait)");
+    return MSF_ERR_TIMEOUT;
+  }
+  float ms = 0;
+  MSF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  res->seconds_raster = 1e-3 * ms;
+  res->seconds_setup = 0;
+  res->probe_slices = n_probes * S;
+  {
+    const int64_t n_batches = (n_probes + B - 1) / B;
+    // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:
+    // 2*S slice passes, the segment sums (chunks, totals) and (pixel modes)
+    // the accumulation
+    res->kernel_launches =
+        P.setup_launches + n_batches * (2 * S + 2 + (P.pix_modes ? 1 : 0));
+  }
+  return finish_raster(ctx, P, ctx->stream, res);
 }
 
 }  // namespace msf

@@ -72,6 +72,48 @@ struct msf_specimen {
 };
 
 namespace msf {
+
+// Device state of one raster over one specimen: the probe, the vacuum-wave
+// tables of split-wave FP32 runs, per-probe pixel shifts, the detector /
+// ring pixel segments and the per-probe sums they fill.  Shared by the
+// batched raster (run_raster) and the slot lanes that mix probes of several
+// rasters (lanes.cpp).
+struct RasterPlan {
+  const msf_specimen* spec = nullptr;
+  msf_optics optics{};
+  msf_detect det{};
+  int64_t n_probes = 0;
+  int S = 0;
+  int64_t plane = 0;
+  bool want_adf = false, pix_modes = false;
+  uint32_t fem = 0;
+  std::vector<int32_t> shifts;  // [n_probes][2] (sx, sy)
+  DevBuf d_shifts;
+  DevBuf probe64;               // normalised probe, real space, FP64
+  DevBuf psi0_tab;              // FP32 runs: [S] vacuum wave entering slice s
+  DevBuf psi0k;                 // FP32 runs: vacuum exit wave, k-space, FP64
+  Rings rings;
+  int n_k = 0, n_seg = 0, n_chunks = 0;
+  DevBuf seg_idx, chunk_begin, seg_chunk;  // segments cut into chunks
+  DevBuf amp, inten;            // [n_probes][n_seg] sums of |psi| and |psi|^2
+  DevBuf acc_a, acc_i;          // [plane] sums over probes (pixel modes)
+  int64_t setup_launches = 0;
+  int64_t device_bytes() const {
+    return (int64_t)(d_shifts.bytes + probe64.bytes + psi0_tab.bytes + psi0k.bytes +
+                     seg_idx.bytes + chunk_begin.bytes + seg_chunk.bytes + amp.bytes +
+                     inten.bytes + acc_a.bytes + acc_i.bytes);
+  }
+};
+// Device bytes plan_raster will allocate (for admission by an HBM budget).
+int64_t raster_plan_bytes(const msf_specimen* spec, bool fp64, int64_t n_probes,
+                          bool pix_modes);
+msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                       const msf_raster* raster, const msf_detect* det, RasterPlan* plan);
+// Copies the plan's sums to the host (synchronising `stream`) and finishes
+// the ADF image and FEM statistics in FP64 in the reference's order.
+msf_status finish_raster(msf_context* ctx, const RasterPlan& plan, cudaStream_t stream,
+                         msf_results* res);
+
 msf_status build_specimen(msf_context* ctx, const msf_grid* grid, const msf_atoms* atoms,
                           msf_specimen* spec);
 msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
@@ -80,4 +122,8 @@ msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_opt
                        DevBuf* probe64);
 msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int reps,
                        double* ms_row, double* ms_col);
+msf_status run_batch(msf_context* ctx, int n, const msf_specimen* const* specs,
+                     const msf_optics* optics, const msf_raster* rasters,
+                     const msf_detect* detects, msf_results* results, int slots);
+int lane_slots(int want, int64_t plane, int lanes, int64_t probes);
 }  // namespace msf

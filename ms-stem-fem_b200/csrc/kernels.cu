@@ -74,6 +74,38 @@ constexpr int col_cols() {
 }
 
 // ------------------------------------------------------------ row pass ---
+// Split-wave transmission step on one row held in registers (element
+// t + T*m of row i).  psi = psi0 + delta with psi0 the probe's vacuum wave
+// (shifted like the probe) and t = 1 + tau.  The reference's update
+// (adfstem.cpp:1929-1949)
+//   re' = (tr*re - ti*im)/s,  im' = (tr*im + ti*re')/s
+// is linear over the reals, so the scattered part evolves as
+//   dre' = (tau_r*p0r - ti*p0i + (1+tau_r)*dre - ti*dim)/s
+//   dim' = (tau_r*p0i + (1+tau_r)*dim + ti*(p0r/s + dre'))/s
+// and every term is formed at the scale of delta, not of psi0.
+template <typename Sh, typename C, typename Real>
+__device__ __forceinline__ void split_update(C (&v)[Sh::E], const C* __restrict__ psi0,
+                                             const C* __restrict__ trans, int nx, int i,
+                                             int t, int sx, int sy, Real is) {
+  constexpr int N = Sh::N, E = Sh::E, T = Sh::T;
+  const int ix = (i < sx) ? i + nx - sx : i - sx;
+  const C* prow = psi0 + (int64_t)ix * N;
+  const C* trow = trans + (int64_t)i * N;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    if (m % kLoadChunk == 0) load_fence();
+    const int y = t + T * m;
+    const int iy = (y < sy) ? y + N - sy : y - sy;
+    const C p0 = __ldg(prow + iy);
+    const C tau = __ldg(trow + y);
+    const C d = v[m];
+    const Real dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
+    const Real re_total = p0.x * is + dre;
+    const Real dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
+    v[m] = C{dre, dim};
+  }
+}
+
 template <typename Real, int N, int LINES, int OP>
 __global__ void __launch_bounds__(LINES * Shape<N, Real>::T,
                                   min_blocks((int)sizeof(Real), LINES * Shape<N, Real>::T))
@@ -96,6 +128,25 @@ row_kernel(const PassArgs a) {
     else __syncthreads();
   };
   C v[E];
+  if constexpr (OP == ROW_SLOTS) {
+    // slot batch: this CTA's probe reads its own slice tables
+    const SlotPass sp = a.slots[b];
+    if (sp.op == SLOT_IDLE) return;
+    if (sp.op == SLOT_FIRST) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; ++m) v[m] = row[t + T * m];
+      fft_line<Sh, true>(v, sm, t, tw, sync);
+    }
+    split_update<Sh>(v, static_cast<const C*>(sp.psi0), static_cast<const C*>(sp.trans), a.nx,
+                     i, t, sp.sx, sp.sy, (Real)a.inv_s);
+    fft_line<Sh, false>(v, sm, t, tw, sync);
+#pragma unroll
+    for (int m = 0; m < E; ++m) row[t + T * m] = v[m];
+    return;
+  }
   if constexpr (OP == ROW_SLICE_FIRST) {
     const int sx = a.shifts[2 * b], sy = a.shifts[2 * b + 1];
     const int ix = (i < sx) ? i + a.nx - sx : i - sx;
@@ -116,31 +167,8 @@ row_kernel(const PassArgs a) {
   }
   if constexpr (OP == ROW_SPLIT || OP == ROW_SPLIT_FIRST) {
     if constexpr (OP == ROW_SPLIT) fft_line<Sh, true>(v, sm, t, tw, sync);
-    // psi = psi0 + delta with psi0 the probe's vacuum wave (shifted like the
-    // probe) and t = 1 + tau.  The reference's update (adfstem.cpp:1929-1949)
-    //   re' = (tr*re - ti*im)/s,  im' = (tr*im + ti*re')/s
-    // is linear over the reals, so the scattered part evolves as
-    //   dre' = (tau_r*p0r - ti*p0i + (1+tau_r)*dre - ti*dim)/s
-    //   dim' = (tau_r*p0i + (1+tau_r)*dim + ti*(p0r/s + dre'))/s
-    // and every term is formed at the scale of delta, not of psi0.
-    const int sx = a.shifts[2 * b], sy = a.shifts[2 * b + 1];
-    const int ix = (i < sx) ? i + a.nx - sx : i - sx;
-    const C* prow = static_cast<const C*>(a.psi0) + (int64_t)ix * N;
-    const C* trow = static_cast<const C*>(a.trans) + (int64_t)i * N;
-    const Real is = (Real)a.inv_s;
-#pragma unroll
-    for (int m = 0; m < E; ++m) {
-      if (m % kLoadChunk == 0) load_fence();
-      const int y = t + T * m;
-      const int iy = (y < sy) ? y + N - sy : y - sy;
-      const C p0 = __ldg(prow + iy);
-      const C tau = __ldg(trow + y);
-      const C d = v[m];
-      const Real dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
-      const Real re_total = p0.x * is + dre;
-      const Real dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
-      v[m] = C{dre, dim};
-    }
+    split_update<Sh>(v, static_cast<const C*>(a.psi0), static_cast<const C*>(a.trans), a.nx, i,
+                     t, a.shifts[2 * b], a.shifts[2 * b + 1], (Real)a.inv_s);
     fft_line<Sh, false>(v, sm, t, tw, sync);
   } else if constexpr (OP == ROW_FWD) {
     fft_line<Sh, false>(v, sm, t, tw, sync);
@@ -189,6 +217,21 @@ col_kernel(const PassArgs a) {
   C* sm = smem + c * SM::stride;
   const C* tw = static_cast<const C*>(a.tw);
   auto sync = [] { __syncthreads(); };
+  // slot batch: this CTA's probe brings its own mask, propagator and step
+  const int32_t* mask_lo = a.mask_lo;
+  const int32_t* mask_hi = a.mask_hi;
+  const void* px_v = a.px;
+  const void* py_v = a.py;
+  [[maybe_unused]] bool stop_in_k = OP == COL_SLICE_LAST;
+  if constexpr (OP == COL_SLOTS) {
+    const SlotPass& sp = a.slots[b];
+    if (sp.op == SLOT_IDLE) return;
+    mask_lo = sp.mask_lo;
+    mask_hi = sp.mask_hi;
+    px_v = sp.px;
+    py_v = sp.py;
+    stop_in_k = sp.last != 0;
+  }
   C v[E];
 #pragma unroll
   for (int m = 0; m < E; ++m) v[m] = col[(int64_t)(t + T * m) * ny];
@@ -200,7 +243,7 @@ col_kernel(const PassArgs a) {
   } else {
     fft_line<Sh, false>(v, sm, t, tw, sync);
     if constexpr (OP != COL_FWD) {
-      const int lo = __ldg(a.mask_lo + j), hi = __ldg(a.mask_hi + j);
+      const int lo = __ldg(mask_lo + j), hi = __ldg(mask_hi + j);
       if constexpr (OP == COL_FWD_MASK_INV) {
 #pragma unroll
         for (int m = 0; m < E; ++m) {
@@ -209,8 +252,8 @@ col_kernel(const PassArgs a) {
         }
       } else {
         const Real is = (Real)a.inv_s;
-        const C pyj = __ldg(static_cast<const C*>(a.py) + j);
-        const C* px = static_cast<const C*>(a.px);
+        const C pyj = __ldg(static_cast<const C*>(py_v) + j);
+        const C* px = static_cast<const C*>(px_v);
 #pragma unroll
         for (int m = 0; m < E; ++m) {
           if (m % kLoadChunk == 0) load_fence();
@@ -225,6 +268,8 @@ col_kernel(const PassArgs a) {
       }
       if constexpr (OP == COL_FWD_MASK_INV || OP == COL_SLICE)
         fft_line<Sh, true>(v, sm, t, tw, sync);
+      if constexpr (OP == COL_SLOTS)
+        if (!stop_in_k) fft_line<Sh, true>(v, sm, t, tw, sync);
     }
   }
 #pragma unroll
@@ -520,6 +565,95 @@ __global__ void segment_reduce_kernel(const double* __restrict__ partial_a,
   }
 }
 
+// ---- slot batches: detection of the slots that finished -------------
+__device__ __forceinline__ const DetectSlot* detect_entries(const void* table) {
+  return reinterpret_cast<const DetectSlot*>(static_cast<const char*>(table) +
+                                             sizeof(DetectTable));
+}
+
+// Work item w = one chunk of one finished slot: the entry is the last one
+// whose chunk_offset <= w (entries without chunks share the next offset).
+__global__ void __launch_bounds__(256)
+slot_chunk_kernel(const void* table, int max_chunks, int nx, int ny, double* partial_a,
+                  double* partial_i) {
+  __shared__ double ra[32], ri[32];
+  const DetectTable* h = static_cast<const DetectTable*>(table);
+  const DetectSlot* e = detect_entries(table);
+  const int n_done = h->n_done, total = h->total_chunks;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int lo = 0, hi = n_done - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (e[mid].chunk_offset <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const DetectSlot& d = e[lo];
+    const int c = w - d.chunk_offset;
+    SplitK sk;
+    sk.psi0k = d.psi0k;
+    sk.nx = nx;
+    sk.ny = ny;
+    double sa = 0.0, si = 0.0;
+    const int s0 = d.chunk_begin[c], s1 = d.chunk_begin[c + 1];
+    for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
+      const double2 v = exit_value<float>(d.psi, __ldg(d.idx + k), sk, d.sx, d.sy);
+      const double i2 = v.x * v.x + v.y * v.y;
+      si += i2;
+      sa += sqrt(i2);
+    }
+    block_sum2(sa, si, ra, ri);
+    if (threadIdx.x == 0) {
+      partial_a[(int64_t)lo * max_chunks + c] = sa;
+      partial_i[(int64_t)lo * max_chunks + c] = si;
+    }
+    __syncthreads();  // ra / ri are reused by the next work item
+  }
+}
+
+// Segment totals of each finished slot, chunk sums added in chunk order.
+__global__ void slot_reduce_kernel(const void* table, int max_chunks,
+                                   const double* __restrict__ partial_a,
+                                   const double* __restrict__ partial_i) {
+  const DetectTable* h = static_cast<const DetectTable*>(table);
+  const DetectSlot* e = detect_entries(table);
+  for (int d = blockIdx.x; d < h->n_done; d += gridDim.x) {
+    const DetectSlot& x = e[d];
+    for (int g = threadIdx.x; g < x.ng; g += blockDim.x) {
+      double sa = 0.0, si = 0.0;
+      for (int c = x.seg_chunk[g]; c < x.seg_chunk[g + 1]; ++c) {
+        sa += partial_a[(int64_t)d * max_chunks + c];
+        si += partial_i[(int64_t)d * max_chunks + c];
+      }
+      x.amp[g] = sa;
+      x.inten[g] = si;
+    }
+  }
+}
+
+// Pixel sums over the finished slots, entries in table order (probes of a
+// raster in raster order), each pixel owned by one thread.
+__global__ void slot_pixel_kernel(const void* table, int nx, int ny) {
+  const DetectTable* h = static_cast<const DetectTable*>(table);
+  const DetectSlot* e = detect_entries(table);
+  const int n_done = h->any_pixel ? h->n_done : 0;
+  const int64_t npix = (int64_t)nx * ny;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix && n_done > 0;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    for (int d = 0; d < n_done; ++d) {
+      const DetectSlot& x = e[d];
+      if (!x.acc_a) continue;
+      SplitK sk;
+      sk.psi0k = x.psi0k;
+      sk.nx = nx;
+      sk.ny = ny;
+      const double2 v = exit_value<float>(x.psi, (int)p, sk, x.sx, x.sy);
+      const double i2 = v.x * v.x + v.y * v.y;
+      x.acc_a[p] += sqrt(i2);
+      x.acc_i[p] += i2;
+    }
+  }
+}
+
 template <typename Real>
 __global__ void pixel_accum_kernel(const Cx<Real>* __restrict__ psi, int64_t stride,
                                    int nb, int64_t npix, double* acc_a, double* acc_i,
@@ -574,6 +708,7 @@ cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s) {
       case ROW_SLICE_FIRST: return row_dispatch<float, ROW_SLICE_FIRST>(a, s);
       case ROW_SPLIT: return row_dispatch<float, ROW_SPLIT>(a, s);
       case ROW_SPLIT_FIRST: return row_dispatch<float, ROW_SPLIT_FIRST>(a, s);
+      case ROW_SLOTS: return row_dispatch<float, ROW_SLOTS>(a, s);
       default: return cudaErrorInvalidValue;  // set-up transforms run in FP64
     }
   }
@@ -593,6 +728,7 @@ cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s) {
     switch (op) {
       case COL_SLICE: return col_dispatch<float, COL_SLICE>(a, s);
       case COL_SLICE_LAST: return col_dispatch<float, COL_SLICE_LAST>(a, s);
+      case COL_SLOTS: return col_dispatch<float, COL_SLOTS>(a, s);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -676,6 +812,24 @@ cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t stride, int 
     if (e != cudaSuccess) return e;
   }
   segment_reduce_kernel<<<nb, 128, 0, s>>>(pa, pi, sp.seg_chunk, sp.ng, sp.n_chunks, amp, inten);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_slot_detect(const void* table, int max_done, int max_chunks, int nx, int ny,
+                               double* partial, bool pixel_sums, cudaStream_t s) {
+  if (max_done <= 0 || max_chunks <= 0) return cudaErrorInvalidValue;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 1;
+  }
+  double* pa = partial;
+  double* pi = partial + (int64_t)max_done * max_chunks;
+  slot_chunk_kernel<<<4 * sms, 256, 0, s>>>(table, max_chunks, nx, ny, pa, pi);
+  slot_reduce_kernel<<<max_done < sms ? max_done : sms, 128, 0, s>>>(table, max_chunks, pa, pi);
+  if (pixel_sums) slot_pixel_kernel<<<2 * sms, 256, 0, s>>>(table, nx, ny);
   return cudaGetLastError();
 }
 

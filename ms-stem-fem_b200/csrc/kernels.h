@@ -19,6 +19,9 @@ enum RowOp : int {
   // integer shift) and the transmission is stored as tau = t - 1.
   ROW_SPLIT = 4,        // iDFT, delta' = Q(t, psi0 + delta) - psi0/s, DFT
   ROW_SPLIT_FIRST = 5,  // delta = 0 on entry: delta' = Q(t, psi0) - psi0/s
+  // Split-wave pass of a slot batch (FP32): every probe reads its own slice
+  // tables and step from PassArgs::slots (ROW_SPLIT_FIRST or ROW_SPLIT).
+  ROW_SLOTS = 6,
 };
 // Which fused operation a column pass (transform along x, strided) does.
 enum ColOp : int {
@@ -27,6 +30,26 @@ enum ColOp : int {
   COL_FWD_MASK_INV = 2,  // forward DFT, band-limit mask, inverse DFT
   COL_SLICE = 3,         // fwd DFT, /s, mask, propagator, inverse DFT
   COL_SLICE_LAST = 4,    // fwd DFT, /s, mask, propagator (stay in k-space)
+  COL_SLOTS = 5,         // COL_SLICE or COL_SLICE_LAST per slot (FP32)
+};
+
+// One probe slot's step in a slot batch: probes of different specimens (of
+// one grid size) share a launch, each at its own slice.
+enum SlotOp : int32_t {
+  SLOT_IDLE = 0,   // empty slot: both passes skip it
+  SLOT_FIRST = 1,  // first slice of a probe (scattered part zero on entry)
+  SLOT_NEXT = 2,   // a later slice
+};
+struct SlotPass {
+  const void* trans = nullptr;       // tau of this slice, [nx][ny] float2
+  const void* psi0 = nullptr;        // vacuum wave entering this slice
+  const void* px = nullptr;          // propagator of this slice along x
+  const void* py = nullptr;          // ... along y
+  const int32_t* mask_lo = nullptr;  // the specimen's band-limit mask
+  const int32_t* mask_hi = nullptr;
+  int32_t op = SLOT_IDLE;
+  int32_t last = 0;                  // 1: last slice, stay in k-space
+  int32_t sx = 0, sy = 0;            // the probe's pixel shift
 };
 
 struct PassArgs {
@@ -50,6 +73,8 @@ struct PassArgs {
   // split-wave row passes: vacuum wave entering this slice, [nx][ny]
   // complex, in the same scale as the inverse-transformed buffer
   const void* psi0 = nullptr;
+  // slot batches (ROW_SLOTS, COL_SLOTS, pipelined column pass): [nb]
+  const SlotPass* slots = nullptr;
 };
 
 // Vacuum part of the exit wave for split-wave detection: k-space values of
@@ -73,8 +98,9 @@ bool pipe_supported(int nx, int ny);
 // Split-wave row pass for slices after the first; *err set to 1 if a copy
 // never arrived (bounded wait).
 cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s);
-// Column slice pass (COL_SLICE, or COL_SLICE_LAST when `last`); `tensor_map`
-// from encode_column_map over the same batch buffer.
+// Column slice pass (COL_SLICE, or COL_SLICE_LAST when `last`; per slot
+// when a.slots is set); `tensor_map` from encode_column_map over the same
+// batch buffer.
 cudaError_t launch_col_slice_pipe(const PassArgs& a, bool last, const void* tensor_map,
                                   int* err, cudaStream_t s);
 // Encode the 2-D tensor map (128 bytes) the column pass loads tiles with.
@@ -126,6 +152,37 @@ struct SegmentPlan {
 cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t batch_stride,
                                 int nb, const SegmentPlan& sp, double* amp, double* inten,
                                 const SplitK& sk, cudaStream_t s);
+// Detection of the slots that finished their last slice in a slot batch.
+struct DetectSlot {
+  const float2* psi = nullptr;         // the slot's exit wave (scattered, k-space)
+  const double* psi0k = nullptr;       // the raster's vacuum exit wave
+  const int32_t* idx = nullptr;        // the raster's segment plan
+  const int32_t* chunk_begin = nullptr;
+  const int32_t* seg_chunk = nullptr;
+  double* amp = nullptr;               // this probe's row of the raster's sums
+  double* inten = nullptr;
+  double* acc_a = nullptr;             // the raster's pixel sums, or nullptr
+  double* acc_i = nullptr;
+  int32_t n_chunks = 0, ng = 0;
+  int32_t sx = 0, sy = 0;
+  int32_t chunk_offset = 0;            // sum of n_chunks over earlier entries
+  int32_t pad = 0;
+};
+// Table the host writes per slot-batch step: `n_done` entries of `done`, in
+// (raster, probe) order so pixel sums add probes in raster order.
+struct DetectTable {
+  int32_t n_done = 0;
+  int32_t total_chunks = 0;
+  int32_t any_pixel = 0;               // some entry has pixel sums
+  int32_t pad = 0;
+};
+// Segment sums and pixel accumulation of the finished slots; `table` points
+// at a DetectTable followed by its DetectSlot entries (device memory), and
+// `partial` holds 2 * max_done * max_chunks doubles.  Fixed grids: the
+// launches can be captured once and replayed with new table contents.
+cudaError_t launch_slot_detect(const void* table, int max_done, int max_chunks, int nx, int ny,
+                               double* partial, bool pixel_sums, cudaStream_t s);
+
 // acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
                                int nb, int64_t npix, double* acc_a, double* acc_i,

@@ -181,7 +181,9 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
 // ----------------------------------------------------- column slice pass --
 constexpr int ctas_per_256(int threads) { return threads >= 256 ? 1 : 256 / threads; }
 
-template <int N, int COLS, bool LAST>
+// SLOTS: every probe of the batch brings its own mask, propagator and step
+// (PassArgs::slots); LAST is then taken per probe from its slot.
+template <int N, int COLS, bool LAST, bool SLOTS>
 __global__ void __launch_bounds__(COLS * Shape<N, float>::T,
                                   ctas_per_256(COLS * Shape<N, float>::T))
 col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap, int* err) {
@@ -235,30 +237,46 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
     parity[w] ^= 1;
     const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
     const int j = g * COLS + c;
-    C* base = bufs + w * BUF;
-    C v[E];
-#pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = base[(t + T * m) * COLS + c];
-    __syncthreads();
-    C* sm = base + c * SM::stride;
-    fft_line<Sh, false>(v, sm, t, tw, sync);
-    const int lo = __ldg(a.mask_lo + j), hi = __ldg(a.mask_hi + j);
-    const C pyj = __ldg(static_cast<const C*>(a.py) + j);
-#pragma unroll
-    for (int m = 0; m < E; ++m) {
-      if (m % kLoadChunk == 0) load_fence();
-      const int i = t + T * m;
-      if (i < lo || i >= hi) {
-        const C p = cmul(__ldg(px + i), pyj);
-        v[m] = cmul(p, cscale(v[m], is));
-      } else {
-        v[m] = C{0.f, 0.f};
-      }
+    const int32_t* mask_lo = a.mask_lo;
+    const int32_t* mask_hi = a.mask_hi;
+    const C* pxb = px;
+    const C* pyb = static_cast<const C*>(a.py);
+    bool idle = false, stop_in_k = LAST;
+    if constexpr (SLOTS) {
+      const SlotPass& sp = a.slots[b];  // uniform over the CTA
+      idle = sp.op == SLOT_IDLE;
+      mask_lo = sp.mask_lo;
+      mask_hi = sp.mask_hi;
+      pxb = static_cast<const C*>(sp.px);
+      pyb = static_cast<const C*>(sp.py);
+      stop_in_k = sp.last != 0;
     }
-    if constexpr (!LAST) fft_line<Sh, true>(v, sm, t, tw, sync);
-    C* col = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + j;
+    if (!idle) {
+      C* base = bufs + w * BUF;
+      C v[E];
 #pragma unroll
-    for (int m = 0; m < E; ++m) col[(int64_t)(t + T * m) * a.ny] = v[m];
+      for (int m = 0; m < E; ++m) v[m] = base[(t + T * m) * COLS + c];
+      __syncthreads();
+      C* sm = base + c * SM::stride;
+      fft_line<Sh, false>(v, sm, t, tw, sync);
+      const int lo = __ldg(mask_lo + j), hi = __ldg(mask_hi + j);
+      const C pyj = __ldg(pyb + j);
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        if (m % kLoadChunk == 0) load_fence();
+        const int i = t + T * m;
+        if (i < lo || i >= hi) {
+          const C p = cmul(__ldg(pxb + i), pyj);
+          v[m] = cmul(p, cscale(v[m], is));
+        } else {
+          v[m] = C{0.f, 0.f};
+        }
+      }
+      if (!stop_in_k) fft_line<Sh, true>(v, sm, t, tw, sync);
+      C* col = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + j;
+#pragma unroll
+      for (int m = 0; m < E; ++m) col[(int64_t)(t + T * m) * a.ny] = v[m];
+    }
     __syncthreads();
     if (threadIdx.x == 0 && item + 2 * (int)gridDim.x < items) {
       fence_proxy_async();
@@ -310,7 +328,7 @@ cudaError_t row_pipe_launch(const PassArgs& a, int* err, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int N, bool LAST>
+template <int N, bool LAST, bool SLOTS = false>
 cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
                             cudaStream_t s) {
   constexpr int CC = pipe_cols<N>();
@@ -318,7 +336,7 @@ cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
   constexpr int RAW = (N * CC > CC * SM::stride ? N * CC : CC * SM::stride);
   constexpr int smem = 2 * ((RAW + 15) / 16 * 16) * 8;
   static int per_sm = 0;
-  auto k = col_slice_pipe_kernel<N, CC, LAST>;
+  auto k = col_slice_pipe_kernel<N, CC, LAST, SLOTS>;
   if (!per_sm) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -362,6 +380,15 @@ cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s) {
 cudaError_t launch_col_slice_pipe(const PassArgs& a, bool last, const void* tensor_map,
                                   int* err, cudaStream_t s) {
   const CUtensorMap& m = *static_cast<const CUtensorMap*>(tensor_map);
+  if (a.slots) {
+    switch (a.nx) {
+      case 256: return col_pipe_launch<256, false, true>(a, m, err, s);
+      case 512: return col_pipe_launch<512, false, true>(a, m, err, s);
+      case 1024: return col_pipe_launch<1024, false, true>(a, m, err, s);
+      case 2048: return col_pipe_launch<2048, false, true>(a, m, err, s);
+    }
+    return cudaErrorInvalidValue;
+  }
   switch (a.nx) {
     case 256: return last ? col_pipe_launch<256, true>(a, m, err, s) : col_pipe_launch<256, false>(a, m, err, s);
     case 512: return last ? col_pipe_launch<512, true>(a, m, err, s) : col_pipe_launch<512, false>(a, m, err, s);

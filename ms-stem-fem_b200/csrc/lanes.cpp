@@ -1,0 +1,259 @@
+// Slot lanes (see lanes.hpp).
+#include "lanes.hpp"
+
+#include <algorithm>
+#include <string>
+
+namespace msf {
+
+namespace {
+
+#define MSF_CUDA(call)                                                      \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) +      \
+                " at " + __FILE__ + ":" + std::to_string(__LINE__));        \
+      return MSF_ERR_CUDA;                                                  \
+    }                                                                       \
+  } while (0)
+
+#define MSF_TRY(call)                \
+  do {                               \
+    msf_status s_ = (call);          \
+    if (s_ != MSF_OK) return s_;     \
+  } while (0)
+
+constexpr size_t round_up(size_t n, size_t a) { return (n + a - 1) / a * a; }
+
+}  // namespace
+
+Lane::Lane(msf_context* ctx, int nx, int ny, int slots)
+    : ctx_(ctx), nx_(nx), ny_(ny), B_(slots), plane_((int64_t)nx * ny) {}
+
+Lane::~Lane() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (graph_) cudaGraphExecDestroy(graph_);
+  for (auto& e : ring_ev_)
+    if (e) cudaEventDestroy(e);
+  if (host_ring_) cudaFreeHost(host_ring_);
+  psi_.release();
+  table_.release();
+  partial_.release();
+  err_.release();
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+msf_status Lane::init() {
+  if (ctx_->fp64) {
+    set_error("slot batches run FP32 wavefields: create the context with MSF_FP32");
+    return MSF_ERR_UNSUPPORTED;
+  }
+  if (B_ <= 0 || !supported_length(nx_) || !supported_length(ny_)) {
+    set_error("invalid lane shape");
+    return MSF_ERR_ARG;
+  }
+  MSF_CUDA(cudaSetDevice(ctx_->device));
+  MSF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  MSF_TRY(ctx_->alloc(&psi_, 8 * (size_t)plane_ * B_));
+  // idle slots are still read by the column pass's tile copies
+  MSF_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, stream_));
+  table_bytes_ = round_up(sizeof(SlotPass) * B_ + sizeof(DetectTable) +
+                              sizeof(DetectSlot) * B_, 256);
+  MSF_TRY(ctx_->alloc(&table_, table_bytes_));
+  MSF_CUDA(cudaMemsetAsync(table_.p, 0, table_bytes_, stream_));
+  MSF_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&host_ring_), kRing * table_bytes_,
+                         cudaHostAllocDefault));
+  for (auto& e : ring_ev_) MSF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  MSF_TRY(ctx_->alloc(&err_, sizeof(int)));
+  MSF_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
+  pipe_col_ = (ctx_->pipe & MSF_PIPE_COL) && pipe_supported(nx_, ny_);
+  if (pipe_col_) MSF_CUDA(encode_column_map(psi_.p, B_, nx_, ny_, col_map_));
+  row_.psi = col_.psi = psi_.p;
+  row_.batch_stride = col_.batch_stride = plane_;
+  row_.nb = col_.nb = B_;
+  row_.nx = col_.nx = nx_;
+  row_.ny = col_.ny = ny_;
+  MSF_TRY(ctx_->twiddles(ny_, false, &row_.tw));
+  MSF_TRY(ctx_->twiddles(nx_, false, &col_.tw));
+  row_.slots = col_.slots = static_cast<const SlotPass*>(table_.p);
+  slot_.assign(B_, Slot{});
+  return MSF_OK;
+}
+
+msf_status Lane::grow_chunks(int n_chunks) {
+  MSF_CUDA(cudaStreamSynchronize(stream_));
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  max_chunks_ = std::max(n_chunks, 1);
+  MSF_TRY(ctx_->alloc(&partial_, sizeof(double) * 2 * (size_t)B_ * max_chunks_));
+  return MSF_OK;
+}
+
+msf_status Lane::add(SlotJob* job) {
+  const Grid& g = job->plan.spec->g;
+  if (g.nx != nx_ || g.ny != ny_) {
+    set_error("raster grid does not match the lane");
+    return MSF_ERR_ARG;
+  }
+  if (job->plan.n_chunks > max_chunks_) MSF_TRY(grow_chunks(job->plan.n_chunks));
+  row_.inv_s = col_.inv_s = 1.0 / g.s;
+  job->next_probe = 0;
+  job->started = job->done = 0;
+  job->complete = false;
+  if (!job->finished) MSF_CUDA(cudaEventCreateWithFlags(&job->finished, cudaEventDisableTiming));
+  queue_.push_back(job);
+  return MSF_OK;
+}
+
+msf_status Lane::launch_step() {
+  MSF_CUDA(launch_row(false, ROW_SLOTS, row_, stream_));
+  if (pipe_col_)
+    MSF_CUDA(launch_col_slice_pipe(col_, false, col_map_, err_.as<int>(), stream_));
+  else
+    MSF_CUDA(launch_col(false, COL_SLOTS, col_, stream_));
+  const char* det = static_cast<const char*>(table_.p) + sizeof(SlotPass) * B_;
+  MSF_CUDA(launch_slot_detect(det, B_, max_chunks_, nx_, ny_, partial_.as<double>(), true,
+                              stream_));
+  return MSF_OK;
+}
+
+msf_status Lane::capture() {
+  cudaGraph_t graph;
+  MSF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  msf_status st = launch_step();
+  cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+  if (st != MSF_OK) return st;
+  MSF_CUDA(ce);
+  MSF_CUDA(cudaGraphInstantiate(&graph_, graph, 0));
+  cudaGraphDestroy(graph);
+  return MSF_OK;
+}
+
+msf_status Lane::step() {
+  if (!busy()) return MSF_OK;
+  // refill idle slots from the queue, oldest raster first
+  for (int i = 0; i < B_ && !queue_.empty(); ++i) {
+    if (slot_[i].job) continue;
+    SlotJob* j = queue_.front();
+    slot_[i].job = j;
+    slot_[i].probe = j->next_probe++;
+    slot_[i].s = 0;
+    ++j->started;
+    ++active_;
+    if (j->next_probe == j->plan.n_probes) queue_.pop_front();
+  }
+
+  // this step's table, in the next free ring entry
+  const int r = (int)(steps_ % kRing);
+  MSF_CUDA(cudaEventSynchronize(ring_ev_[r]));
+  unsigned char* h = host_ring_ + (size_t)r * table_bytes_;
+  SlotPass* sp = reinterpret_cast<SlotPass*>(h);
+  DetectTable* dt = reinterpret_cast<DetectTable*>(h + sizeof(SlotPass) * B_);
+  DetectSlot* de = reinterpret_cast<DetectSlot*>(dt + 1);
+  std::vector<int> done;
+  for (int i = 0; i < B_; ++i) {
+    const Slot& sl = slot_[i];
+    SlotPass p;
+    if (sl.job) {
+      const RasterPlan& P = sl.job->plan;
+      const msf_specimen* spec = P.spec;
+      p.op = sl.s == 0 ? SLOT_FIRST : SLOT_NEXT;
+      p.last = sl.s + 1 == P.S;
+      p.trans = static_cast<const char*>(spec->t.p) + 8 * plane_ * sl.s;
+      p.psi0 = static_cast<const char*>(P.psi0_tab.p) + 8 * plane_ * sl.s;
+      p.px = static_cast<const char*>(spec->prop.p) + 8 * (size_t)(nx_ + ny_) * sl.s;
+      p.py = static_cast<const char*>(p.px) + 8 * (size_t)nx_;
+      p.mask_lo = spec->mask_lo.as<int32_t>();
+      p.mask_hi = spec->mask_hi.as<int32_t>();
+      p.sx = P.shifts[2 * sl.probe];
+      p.sy = P.shifts[2 * sl.probe + 1];
+      if (p.last) done.push_back(i);
+    }
+    sp[i] = p;
+  }
+  // detection entries in (raster, probe) order
+  std::sort(done.begin(), done.end(), [&](int a, int b) {
+    const Slot &x = slot_[a], &y = slot_[b];
+    if (x.job->order != y.job->order) return x.job->order < y.job->order;
+    return x.probe < y.probe;
+  });
+  DetectTable t;
+  t.n_done = (int32_t)done.size();
+  for (size_t k = 0; k < done.size(); ++k) {
+    const Slot& sl = slot_[done[k]];
+    const RasterPlan& P = sl.job->plan;
+    DetectSlot e;
+    e.psi = psi_.as<float2>() + plane_ * done[k];
+    e.psi0k = P.psi0k.as<double>();
+    e.idx = P.seg_idx.as<int32_t>();
+    e.chunk_begin = P.chunk_begin.as<int32_t>();
+    e.seg_chunk = P.seg_chunk.as<int32_t>();
+    e.amp = P.amp.as<double>() + sl.probe * P.n_seg;
+    e.inten = P.inten.as<double>() + sl.probe * P.n_seg;
+    if (P.pix_modes) {
+      e.acc_a = P.acc_a.as<double>();
+      e.acc_i = P.acc_i.as<double>();
+      t.any_pixel = 1;
+    }
+    e.n_chunks = P.n_chunks;
+    e.ng = P.n_seg;
+    e.sx = P.shifts[2 * sl.probe];
+    e.sy = P.shifts[2 * sl.probe + 1];
+    e.chunk_offset = t.total_chunks;
+    t.total_chunks += P.n_chunks;
+    de[k] = e;
+  }
+  *dt = t;
+  MSF_CUDA(cudaMemcpyAsync(table_.p, h, table_bytes_, cudaMemcpyHostToDevice, stream_));
+  MSF_CUDA(cudaEventRecord(ring_ev_[r], stream_));
+
+  // the first step runs its launches directly (kernel attributes are set
+  // on first use); later steps replay the captured graph
+  if (ctx_->graphs && steps_ >= 1 && !graph_) MSF_TRY(capture());
+  if (graph_) {
+    MSF_CUDA(cudaGraphLaunch(graph_, stream_));
+  } else {
+    MSF_TRY(launch_step());
+  }
+  launches_ += 5;
+  ++steps_;
+
+  // advance every active slot by one slice
+  for (int i = 0; i < B_; ++i) {
+    Slot& sl = slot_[i];
+    if (!sl.job) continue;
+    if (sl.s + 1 == sl.job->plan.S) {
+      SlotJob* j = sl.job;
+      if (++j->done == j->plan.n_probes) {
+        MSF_CUDA(cudaEventRecord(j->finished, stream_));
+        j->complete = true;
+      }
+      sl = Slot{};
+      --active_;
+    } else {
+      ++sl.s;
+    }
+  }
+  return MSF_OK;
+}
+
+msf_status Lane::synchronize() {
+  MSF_CUDA(cudaStreamSynchronize(stream_));
+  return MSF_OK;
+}
+
+msf_status Lane::check_error() {
+  int flag = 0;
+  MSF_CUDA(cudaMemcpyAsync(&flag, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  MSF_CUDA(cudaStreamSynchronize(stream_));
+  if (flag) {
+    set_error("a pipelined slice pass gave up waiting for a tile copy (bounded wait)");
+    return MSF_ERR_TIMEOUT;
+  }
+  return MSF_OK;
+}
+
+}  // namespace msf

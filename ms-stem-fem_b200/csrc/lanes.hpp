@@ -1,0 +1,98 @@
+// Slot lanes: continuous batching of probes from several rasters.
+//
+// A lane owns `slots` FP32 wavefields of one grid size.  Every step runs one
+// row pass and one column pass over all slots, each slot at its own slice of
+// its own raster (specimen, probe, shift), then the detection of the slots
+// that just finished their last slice.  A finished slot is refilled at the
+// next step with the next waiting probe of any raster of that grid size, so
+// rasters that arrive while others run join the same launches.
+//
+// Per step the host writes one table (SlotPass per slot, then the
+// detection entries) into a pinned ring and copies it to a fixed device
+// table; the three launches of a step read only that table, so they are
+// captured once as a CUDA graph and replayed.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <deque>
+#include <memory>
+#include <vector>
+
+#include "engine.hpp"
+#include "kernels.h"
+
+namespace msf {
+
+// One raster taking part in slot batches.
+struct SlotJob {
+  RasterPlan plan;
+  uint64_t order = 0;          // admission order: detection entries sort by it
+  int64_t next_probe = 0;      // next probe to start
+  int64_t started = 0, done = 0;
+  cudaEvent_t finished = nullptr;  // recorded after the last detection
+  bool complete = false;       // `finished` has been recorded
+  ~SlotJob() {
+    if (finished) cudaEventDestroy(finished);
+  }
+};
+
+class Lane {
+ public:
+  Lane(msf_context* ctx, int nx, int ny, int slots);
+  ~Lane();
+  Lane(const Lane&) = delete;
+  Lane& operator=(const Lane&) = delete;
+
+  msf_status init();
+  // The job's probes join the lane's queue (the job must outlive the lane's
+  // use of it: until it is complete and the lane has synchronised).
+  msf_status add(SlotJob* job);
+  bool busy() const { return active_ > 0 || !queue_.empty(); }
+  // True when step() would not wait for a free table in the ring.
+  bool ready() const {
+    return cudaEventQuery(ring_ev_[steps_ % kRing]) != cudaErrorNotReady;
+  }
+  // Plans and enqueues one step; no-op when idle.
+  msf_status step();
+  msf_status synchronize();
+  // 0, or 1 when a pipelined pass gave up on a tile copy (bounded wait).
+  msf_status check_error();
+  cudaStream_t stream() const { return stream_; }
+  int nx() const { return nx_; }
+  int ny() const { return ny_; }
+  int slots() const { return B_; }
+  int64_t steps() const { return steps_; }
+  int64_t launches() const { return launches_; }
+
+ private:
+  struct Slot {
+    SlotJob* job = nullptr;
+    int64_t probe = -1;
+    int s = 0;
+  };
+  msf_status capture();
+  msf_status launch_step();
+  msf_status grow_chunks(int n_chunks);
+
+  msf_context* ctx_;
+  int nx_, ny_, B_;
+  int64_t plane_;
+  cudaStream_t stream_ = nullptr;
+  DevBuf psi_, table_, partial_, err_;
+  int max_chunks_ = 0;
+  bool pipe_col_ = false;
+  alignas(64) unsigned char col_map_[128];
+  PassArgs row_, col_;
+  size_t table_bytes_ = 0;
+  static constexpr int kRing = 4;
+  unsigned char* host_ring_ = nullptr;  // kRing pinned tables
+  cudaEvent_t ring_ev_[kRing] = {};
+  cudaGraphExec_t graph_ = nullptr;
+  std::vector<Slot> slot_;
+  std::deque<SlotJob*> queue_;
+  int active_ = 0;
+  int64_t steps_ = 0, launches_ = 0;
+  bool any_pixel_jobs_ = false;
+};
+
+}  // namespace msf

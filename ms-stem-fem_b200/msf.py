@@ -40,6 +40,8 @@ EXPORTED = [
     "msf_job_destroy", "msf_job_describe", "msf_job_output_prefix",
     "msf_read_specimen", "msf_write_outputs", "msf_main", "msf_slice_atoms",
     "msf_time_passes", "msf_context_transfer_bytes", "msf_probe_noalloc",
+    "msf_run_batch", "msf_server_create", "msf_server_submit", "msf_server_poll",
+    "msf_server_stats_get", "msf_server_destroy",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -90,6 +92,19 @@ class Results(C.Structure):
                 ("seconds_raster", C.c_double)]
 
 
+class Request(C.Structure):
+    _fields_ = [("grid", Grid), ("atoms", Atoms), ("optics", Optics), ("raster", Raster),
+                ("detect", Detect)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("running", C.c_int64), ("waiting", C.c_int64), ("p50_s", C.c_double),
+                ("p99_s", C.c_double), ("max_s", C.c_double),
+                ("probe_slices_per_s", C.c_double), ("probe_slices", C.c_int64),
+                ("device_bytes", C.c_int64)]
+
+
 class MsfError(RuntimeError):
     def __init__(self, status, message):
         super().__init__("msf status %d: %s" % (status, message))
@@ -138,6 +153,14 @@ def lib() -> C.CDLL:
         L.msf_read_specimen.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
         L.msf_write_outputs.argtypes = [C.c_void_p, C.POINTER(Results)]
         L.msf_main.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(Options)]
+        L.msf_run_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p),
+                                    C.POINTER(Optics), C.POINTER(Raster), C.POINTER(Detect),
+                                    C.POINTER(Results), C.c_int32]
+        L.msf_server_create.argtypes = [C.POINTER(Options), C.c_int32, C.POINTER(C.c_void_p)]
+        L.msf_server_submit.argtypes = [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]
+        L.msf_server_poll.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(Results)]
+        L.msf_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.msf_server_destroy.argtypes = [C.c_void_p]
         L.msf_slice_atoms.argtypes = [C.c_int64, _dp, C.c_double, C.c_double, C.c_double,
                                       _ip, _dp, _dp, _lp, _lp, C.c_int32]
         L.msf_context_transfer_bytes.argtypes = [C.c_void_p, _lp, _lp, C.c_int32]
@@ -281,6 +304,29 @@ class Context:
         out.finish(raster, detect)
         return out
 
+    def run_batch(self, jobs, slots=0, want_means=False, want_rings=False, cap_k=8192):
+        """Several rasters through slot lanes (msf_run_batch).
+
+        jobs: sequence of (Specimen, Optics, Raster, Detect); returns one
+        RunResult per job, as ``run`` would (without the final wave)."""
+        n = len(jobs)
+        specs = (C.c_void_p * n)(*[j[0]._h.value for j in jobs])
+        optics = (Optics * n)(*[j[1] for j in jobs])
+        rasters = (Raster * n)(*[j[2] for j in jobs])
+        detects = (Detect * n)(*[j[3] for j in jobs])
+        outs = []
+        for spec, _, raster, _ in jobs:
+            ck = min(cap_k, 1024) if want_rings else cap_k
+            outs.append(RunResult(raster.n_x * raster.n_y, ck, spec.grid.nx, spec.grid.ny,
+                                  False, want_means, want_rings))
+        structs = (Results * n)(*[o._struct for o in outs])
+        _check(lib().msf_run_batch(self._h, n, specs, optics, rasters, detects, structs,
+                                   slots))
+        for k, (o, j) in enumerate(zip(outs, jobs)):
+            o._struct = structs[k]
+            o.finish(j[2], j[3])
+        return outs
+
     def time_passes(self, spec: "Specimen", nb: int, reps: int = 10):
         """Mean ms per launch of the fused row and column slice passes."""
         r, c = C.c_double(), C.c_double()
@@ -291,6 +337,53 @@ class Context:
         out = np.zeros(2 * spec.grid.nx * spec.grid.ny)
         _check(lib().msf_probe(self._h, spec._h, C.byref(optics), _p(out)))
         return out.reshape(spec.grid.nx, spec.grid.ny, 2)
+
+
+class Server:
+    """Request loop with continuous batching (msf_server_*), FP32 wavefields."""
+
+    def __init__(self, device=0, slots=0, hbm_budget=0, graphs=True):
+        opt = Options(device, MSF_FP32, 0, 1 if graphs else 0, hbm_budget)
+        h = C.c_void_p()
+        _check(lib().msf_server_create(C.byref(opt), slots, C.byref(h)))
+        self._h = h
+        self._pending = {}
+
+    def submit(self, grid: Grid, q, z, optics: Optics, raster: Raster, detect: Detect) -> int:
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
+        z = np.ascontiguousarray(z, dtype=np.uint32)
+        req = Request(grid, Atoms(len(z), _p(q), z.ctypes.data_as(C.POINTER(C.c_uint32))),
+                      optics, raster, detect)
+        t = C.c_uint64()
+        _check(lib().msf_server_submit(self._h, C.byref(req), C.byref(t)))
+        self._pending[t.value] = (grid.nx, grid.ny, raster, detect)
+        return t.value
+
+    def poll(self, ticket: int, wait_ms=0, want_means=False, want_rings=False, cap_k=8192):
+        """RunResult when finished, None while queued or running."""
+        nx, ny, raster, detect = self._pending[ticket]
+        ck = min(cap_k, 1024) if want_rings else cap_k
+        out = RunResult(raster.n_x * raster.n_y, ck, nx, ny, False, want_means, want_rings)
+        st = lib().msf_server_poll(self._h, ticket, int(wait_ms), C.byref(out._struct))
+        if st == 8:  # MSF_ERR_BUSY
+            return None
+        del self._pending[ticket]
+        _check(st)
+        out.finish(raster, detect)
+        return out
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().msf_server_stats_get(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().msf_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 class Specimen:

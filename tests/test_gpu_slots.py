@@ -1,0 +1,142 @@
+"""Slot batches (msf_run_batch) and the request loop (msf_server_*).
+
+Each probe in a slot batch runs the same arithmetic as in a plain batched
+raster, only its launch companions differ (probes of other rasters, at other
+slices), so:
+  * every raster of a mixed batch matches its own msf_run within FP32
+    rounding (ADF image and V(k) to 1e-6 relative, V(k) floor 1e-9);
+  * a request served in a mix returns exactly what it returns alone
+    (bit-identical: detection sums run in raster order either way).
+"""
+import time
+
+import numpy as np
+import pytest
+
+import msf
+import specimen
+from conftest import assert_variance_close, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FEM = msf.OUT_ADF_IMAGE | msf.OUT_V_OMEGA | msf.OUT_VBAR_R | msf.OUT_V_RE | msf.OUT_V_GT17
+MODES = ["V_omega", "Vbar_r", "V_re", "V_gt17"]
+
+
+class JobSpec:
+    """A small seeded amorphous-Si raster (arrays kept alive with the structs)."""
+
+    def __init__(self, n, box, zbox, n_atoms, seed, raster_n, outputs=FEM, defocus=400.0):
+        self.pos = specimen.amorphous_positions(n_atoms, (box, box, zbox), seed=seed)
+        self.z = np.full(n_atoms, 14, dtype=np.uint32)
+        self.grid = msf.Grid(nx=n, ny=n, voltage=200000.0, xperiod=box, yperiod=box,
+                             zperiod=zbox, dupe_x=1, dupe_y=1, dupe_z=1, replicate_atoms=0,
+                             xmin=0.0, ymin=0.0, zmin=0.0, min_slice=2.0)
+        self.optics = msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0, defocus=defocus,
+                                 alpha_max=0.010)
+        self.xp = np.arange(raster_n) * (box / raster_n)
+        self.raster = msf.Raster(raster_n, raster_n, self.xp.ctypes.data_as(msf._dp),
+                                 self.xp.ctypes.data_as(msf._dp))
+        self.detect = msf.Detect(outputs=outputs, det_inner=0.04, det_outer=0.2, dr=1.0)
+
+
+def jobs_mixed():
+    return [
+        JobSpec(256, 25.0, 20.0, 600, seed=11, raster_n=6),
+        JobSpec(128, 12.5, 14.0, 100, seed=12, raster_n=5),   # plain column pass
+        JobSpec(256, 25.0, 30.0, 900, seed=13, raster_n=4, defocus=0.0),
+        JobSpec(512, 50.0, 8.0, 900, seed=14, raster_n=3),
+        JobSpec(256, 25.0, 10.0, 300, seed=15, raster_n=5, outputs=msf.OUT_ADF_IMAGE),
+    ]
+
+
+def assert_same_run(a, b, rtol, atol, what):
+    err = rel_err(a.adf_image, b.adf_image)
+    m = np.abs(b.adf_image) > 0
+    if m.any():
+        assert err[m].max() <= rtol, (what, "ADF", err[m].max())
+    assert a.n_k == b.n_k, what
+    for mode, v in b.v.items():
+        assert_variance_close(a.v[mode], v, rtol, atol, what="%s %s" % (what, mode))
+
+
+@pytest.mark.parametrize("slots", [0, 7])
+def test_batch_matches_single_runs(slots):
+    ctx = msf.Context(precision="fp32", batch=16)
+    js = jobs_mixed()
+    specs = [ctx.specimen(j.grid, j.pos, j.z) for j in js]
+    singles = [ctx.run(s, j.optics, j.raster, j.detect) for s, j in zip(specs, js)]
+    outs = ctx.run_batch([(s, j.optics, j.raster, j.detect) for s, j in zip(specs, js)],
+                         slots=slots)
+    for k, (o, r) in enumerate(zip(outs, singles)):
+        assert o.probe_slices == r.probe_slices
+        assert_same_run(o, r, 1e-6, 1e-9, "job %d slots %d" % (k, slots))
+
+
+def test_batch_rejects_fp64_context():
+    ctx = msf.Context(precision="fp64")
+    j = jobs_mixed()[1]
+    s = ctx.specimen(j.grid, j.pos, j.z)
+    with pytest.raises(msf.MsfError):
+        ctx.run_batch([(s, j.optics, j.raster, j.detect)])
+
+
+def serve(jobs, slots, stagger_s=0.0):
+    srv = msf.Server(slots=slots)
+    tickets = []
+    for j in jobs:
+        tickets.append(srv.submit(j.grid, j.pos, j.z, j.optics, j.raster, j.detect))
+        if stagger_s:
+            time.sleep(stagger_s)
+    outs = []
+    for t in tickets:
+        r = None
+        deadline = time.time() + 300
+        while r is None:
+            assert time.time() < deadline, "request did not finish"
+            r = srv.poll(t, wait_ms=200)
+        outs.append(r)
+    stats = srv.stats()
+    srv.close()
+    return outs, stats
+
+
+def test_server_result_same_alone_and_in_mix():
+    js = jobs_mixed()
+    alone = [serve([j], slots=5)[0][0] for j in js]
+    mixed, stats = serve(js, slots=5, stagger_s=0.01)
+    for k, (a, b) in enumerate(zip(mixed, alone)):
+        assert np.array_equal(a.adf_image, b.adf_image), k
+        for mode in b.v:
+            assert np.array_equal(a.v[mode], b.v[mode], equal_nan=True), (k, mode)
+    assert stats["completed"] == len(js) and stats["failed"] == 0
+    assert 0 < stats["p50_s"] <= stats["p99_s"] <= stats["max_s"]
+
+
+def test_server_matches_plain_run():
+    ctx = msf.Context(precision="fp32")
+    js = jobs_mixed()[:2]
+    outs, _ = serve(js, slots=3)
+    for k, (o, j) in enumerate(zip(outs, js)):
+        s = ctx.specimen(j.grid, j.pos, j.z)
+        r = ctx.run(s, j.optics, j.raster, j.detect)
+        assert_same_run(o, r, 1e-6, 1e-9, "served job %d" % k)
+
+
+def test_server_reports_request_errors():
+    srv = msf.Server(slots=4)
+    j = jobs_mixed()[1]
+    bad = msf.Grid.from_buffer_copy(j.grid)
+    bad.nx = 100  # not a power of two
+    t = srv.submit(bad, j.pos, j.z, j.optics, j.raster, j.detect)
+    good = srv.submit(j.grid, j.pos, j.z, j.optics, j.raster, j.detect)
+    with pytest.raises(msf.MsfError):
+        while srv.poll(t, wait_ms=200) is None:
+            pass
+    r = None
+    while r is None:
+        r = srv.poll(good, wait_ms=200)
+    assert r.probe_slices > 0
+    st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == 1
+    srv.close()
