@@ -17,9 +17,12 @@ results back.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun each rank runs its own replica of the job on its GPU (the
-probes are independent; there is no data-path collective), so scaling is
-weak; rank 0 prints one JSON line.
+Under torchrun (N ranks, one per GPU) the raster grows to (64 N) x 64 probes
+(x spacing / N) and is sharded: each rank runs its contiguous 4,096 probes,
+then the one exchange step all-gathers the per-probe detector rows and the
+per-pixel sums over NCCL and every rank finishes the FEM statistics.  Work
+per GPU is fixed, so scaling is weak; a step is timed with CUDA events around
+shard + exchange + finish, max over ranks; rank 0 prints one JSON line.
 """
 import argparse
 import json
@@ -283,18 +286,47 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    if world > 1:
+        # weak scaling: one raster of (64 N) x 64 probes (x spacing / N); each
+        # rank runs its contiguous 4,096 probes, then the per-probe rows and
+        # pixel sums are exchanged and every rank finishes the FEM statistics
+        import shards
+        import torch
+        n_x = job.raster.n_x * world
+        xp_w = np.arange(n_x) * (job.grid.xperiod / n_x)
+        yp_w = np.array(job.raster.y_p[:job.raster.n_y])
+        raster_w = msf.Raster(n_x, job.raster.n_y, xp_w.ctypes.data_as(msf._dp),
+                              yp_w.ctypes.data_as(msf._dp))
+
+        def step():
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            res, part = shards.run_sharded(ctx, spec, job.optics, raster_w, job.detect, rank,
+                                           world, dist, device="cuda")
+            ev1.record()
+            torch.cuda.synchronize()
+            return res, part, 1e-3 * ev0.elapsed_time(ev1)
     for _ in range(args.warmup):
-        ctx.run(spec, job.optics, job.raster, job.detect)
+        if world > 1:
+            step()
+        else:
+            ctx.run(spec, job.optics, job.raster, job.detect)
     barrier()
     dev_times, launches, ps = [], 0, 0
     with ClockSampler(local) as clocks:
         wall0 = time.time()
         for _ in range(args.steps):
-            r = ctx.run(spec, job.optics, job.raster, job.detect)
+            if world > 1:
+                r, part, t_step = step()
+                dev_times.append(t_step)
+                launches += part.get("kernel_launches", 0)
+                ps += part["probe_slices"]
+            else:
+                r = ctx.run(spec, job.optics, job.raster, job.detect)
+                dev_times.append(r.seconds_raster)
+                launches += r.kernel_launches
+                ps += r.probe_slices
             last = r
-            dev_times.append(r.seconds_raster)
-            launches += r.kernel_launches
-            ps += r.probe_slices
         wall = time.time() - wall0
     barrier()
     total_dev = sum(dev_times)
@@ -303,7 +335,7 @@ def main():
         t = torch.tensor([total_dev], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_dev = float(t.item())
-    value = ps * world / total_dev
+    value = ps * world / total_dev  # ps: this rank's probe*slices (equal shards)
     ms_per_step = 1e3 * total_dev / args.steps
 
     # roofline of the dominant kernel (fused row / column slice pass)
@@ -334,8 +366,13 @@ def main():
         e2e_ps = 0
         for _ in range(e2e_steps):
             s2 = ctx.specimen(job.grid, q, z)
-            r2 = ctx.run(s2, job.optics, job.raster, job.detect)
-            e2e_ps += r2.probe_slices
+            if world > 1:
+                _, p2 = shards.run_sharded(ctx, s2, job.optics, raster_w, job.detect, rank,
+                                           world, dist, device="cuda")
+                e2e_ps += p2["probe_slices"]
+            else:
+                r2 = ctx.run(s2, job.optics, job.raster, job.detect)
+                e2e_ps += r2.probe_slices
             s2.close()
         e2e_t = time.time() - t0
         h2d, d2h = ctx.transfer_bytes(reset=True)
@@ -379,7 +416,10 @@ def main():
                                        "64x64 raster, %d slices" % n_slices,
                            "probes": job.n_probes, "slices": n_slices,
                            "probe_slices_per_step": ps // args.steps,
-                           "parallelism": "replica per GPU (probes independent)",
+                           "parallelism": ("one raster of %dx64 probes sharded over %d GPUs, "
+                                           "per-probe rows all-gathered for the FEM finish"
+                                           % (64 * world, world)) if world > 1 else
+                                          "1 GPU",
                            "l2": "inputs exceed L2: %.0f MB of transmission functions" %
                                  (spec.device_bytes() / 1e6),
                            "graphs": not args.no_graphs, "batch": args.batch or "auto",

@@ -184,6 +184,35 @@ msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
 msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
                              double* probe_device, void* stream);
 
+/* ---- one raster sharded over several GPUs ------------------------------ */
+/* The reference splits a raster over MPI ranks and reduces the detector
+ * sums with MPI_Reduce / MPI_Allgatherv (adfstem.cpp:1556-1606, 2489-2782,
+ * 2822-3612).  Here each GPU runs a contiguous range of probes with
+ * msf_run_partial, the caller exchanges the per-probe rows (all-gather, in
+ * probe order) and the per-pixel sums (sum), and any rank finishes with
+ * msf_finish, which needs no GPU. */
+/* Segments per probe: FEM ring bins, then the ADF annulus (n_k + 1). */
+int32_t msf_segment_count(const msf_grid* grid, const msf_detect* detect);
+/* Probes [p_begin, p_end) of the raster (pixel snaps found over the whole
+ * raster, as the reference's carried-over search needs).  amp / inten get
+ * (p_end - p_begin) rows of msf_segment_count doubles: per segment the sum
+ * of |psi(k)| and of |psi(k)|^2; acc_a / acc_i (pixel FEM modes) nx*ny sums
+ * of |psi(k)| and |psi(k)|^2 over these probes.  Any output may be NULL.
+ * `info` (may be NULL) receives probe_slices, kernel_launches, n_k and
+ * seconds_raster. */
+msf_status msf_run_partial(msf_context* ctx, const msf_specimen* spec,
+                           const msf_optics* optics, const msf_raster* raster,
+                           const msf_detect* detect, int64_t p_begin, int64_t p_end,
+                           double* amp, double* inten, double* acc_a, double* acc_i,
+                           msf_results* info);
+/* ADF image and FEM statistics of a whole raster from the rows of all its
+ * probes in raster order and the summed pixel sums (host only; the same
+ * arithmetic as msf_run's finish). */
+msf_status msf_finish(const msf_grid* grid, const msf_optics* optics,
+                      const msf_detect* detect, int64_t n_probes, const double* amp,
+                      const double* inten, const double* acc_a, const double* acc_i,
+                      msf_results* results);
+
 /* ---- slot batches and serving (no counterpart in the reference) -------- */
 /* Several rasters at once: results[i] is what msf_run(ctx, specs[i],
  * &optics[i], &rasters[i], &detects[i], &results[i]) returns, within FP32

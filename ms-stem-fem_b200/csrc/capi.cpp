@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "kernels.h"
 #include "msf.h"
 #include "setup.hpp"
 
@@ -190,6 +191,43 @@ msf_status msf_run(msf_context* ctx, const msf_specimen* spec, const msf_optics*
     return MSF_ERR_ARG;
   }
   return run_raster(ctx, spec, optics, raster, detect, results);
+}
+
+int32_t msf_segment_count(const msf_grid* grid, const msf_detect* detect) {
+  if (!grid || !detect) return -1;
+  if (!(detect->outputs & MSF_OUT_FEM_MASK)) return 1;
+  Grid g = grid_of(grid);
+  return make_rings(g, detect->dr).n_k + 1;
+}
+
+msf_status msf_run_partial(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                           const msf_raster* raster, const msf_detect* detect, int64_t p_begin,
+                           int64_t p_end, double* amp, double* inten, double* acc_a,
+                           double* acc_i, msf_results* info) {
+  if (!ctx || !spec || spec->ctx != ctx) {
+    set_error("specimen does not belong to this context");
+    return MSF_ERR_ARG;
+  }
+  return run_partial(ctx, spec, optics, raster, detect, p_begin, p_end, amp, inten, acc_a,
+                     acc_i, info);
+}
+
+msf_status msf_finish(const msf_grid* grid, const msf_optics* optics, const msf_detect* detect,
+                      int64_t n_probes, const double* amp, const double* inten,
+                      const double* acc_a, const double* acc_i, msf_results* results) {
+  if (!grid || !optics || !detect || !results || n_probes <= 0 || !inten ||
+      ((detect->outputs & MSF_OUT_FEM_MASK) && !amp)) {
+    set_error("msf_finish: null argument or empty raster");
+    return MSF_ERR_ARG;
+  }
+  if (!supported_length(grid->nx) || !supported_length(grid->ny)) {
+    set_error("unsupported grid");
+    return MSF_ERR_UNSUPPORTED;
+  }
+  Grid g = grid_of(grid);
+  Rings rings;
+  if (detect->outputs & MSF_OUT_FEM_MASK) rings = make_rings(g, detect->dr);
+  return finish_host(g, rings, *optics, *detect, n_probes, amp, inten, acc_a, acc_i, results);
 }
 
 msf_status msf_run_batch(msf_context* ctx, int32_t n, const msf_specimen* const* specs,

@@ -424,7 +424,8 @@ int64_t raster_plan_bytes(const msf_specimen* spec, bool fp64, int64_t n_probes,
 }
 
 msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
-                       const msf_raster* raster, const msf_detect* det, RasterPlan* P) {
+                       const msf_raster* raster, const msf_detect* det, RasterPlan* P,
+                       int64_t p_begin, int64_t p_end) {
   if (!spec || !optics || !raster || !det || !P) { set_error("null argument"); return MSF_ERR_ARG; }
   const Grid& g = spec->g;
   const int64_t plane = (int64_t)g.nx * g.ny;
@@ -433,9 +434,18 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
   if (S <= 0) { set_error("specimen has no slices"); return MSF_ERR_ARG; }
   std::vector<double> x_p(raster->x_p, raster->x_p + std::max(0, raster->n_x));
   std::vector<double> y_p(raster->y_p, raster->y_p + std::max(0, raster->n_y));
-  const int64_t n_probes = (int64_t)x_p.size() * (int64_t)y_p.size();
-  if (n_probes <= 0) { set_error("empty raster"); return MSF_ERR_ARG; }
+  const int64_t n_all = (int64_t)x_p.size() * (int64_t)y_p.size();
+  if (n_all <= 0) { set_error("empty raster"); return MSF_ERR_ARG; }
+  if (p_end < 0) p_end = n_all;
+  if (p_begin < 0 || p_begin >= p_end || p_end > n_all) {
+    set_error("probe range [" + std::to_string(p_begin) + ", " + std::to_string(p_end) +
+              ") outside the raster's " + std::to_string(n_all) + " probes");
+    return MSF_ERR_ARG;
+  }
+  const int64_t n_probes = p_end - p_begin;
   P->spec = spec;
+  P->p_begin = p_begin;
+  P->n_raster = n_all;
   P->optics = *optics;
   P->det = *det;
   P->n_probes = n_probes;
@@ -498,11 +508,15 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
     MSF_CUDA(cudaStreamSynchronize(ctx->stream));
   }
 
-  // per-probe pixel shifts
+  // per-probe pixel shifts: the reference's search carries its position
+  // over from probe to probe, so they are found over the whole raster and
+  // the range's slice is kept
   if (!probe_shifts(g, x_p, y_p, &P->shifts)) {
     set_error("a raster position lies half a pixel or more below the cell origin");
     return MSF_ERR_ARG;
   }
+  P->shifts = std::vector<int32_t>(P->shifts.begin() + 2 * p_begin,
+                                   P->shifts.begin() + 2 * p_end);
   MSF_TRY(upload(ctx, &P->d_shifts, P->shifts));
 
   // segments: ring bins (FEM) then the ADF detector annulus
@@ -544,43 +558,70 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
   return MSF_OK;
 }
 
+msf_status download_sums(msf_context* ctx, const RasterPlan& P, cudaStream_t stream,
+                         double* amp, double* inten, double* acc_a, double* acc_i) {
+  const size_t rows = (size_t)P.n_probes * P.n_seg;
+  if (amp)
+    MSF_CUDA(cudaMemcpyAsync(amp, P.amp.p, rows * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream));
+  if (inten)
+    MSF_CUDA(cudaMemcpyAsync(inten, P.inten.p, rows * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream));
+  if (P.pix_modes && acc_a)
+    MSF_CUDA(cudaMemcpyAsync(acc_a, P.acc_a.p, P.plane * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream));
+  if (P.pix_modes && acc_i)
+    MSF_CUDA(cudaMemcpyAsync(acc_i, P.acc_i.p, P.plane * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream));
+  MSF_CUDA(cudaStreamSynchronize(stream));
+  ctx->d2h_bytes += (int64_t)(((amp ? 1 : 0) + (inten ? 1 : 0)) * rows * sizeof(double)) +
+                    (P.pix_modes ? ((acc_a ? 8 : 0) + (acc_i ? 8 : 0)) * P.plane : 0);
+  return MSF_OK;
+}
+
 msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t stream,
                          msf_results* res) {
-  const Grid& g = P.spec->g;
-  const int64_t plane = P.plane, n_probes = P.n_probes;
-  const int n_k = P.n_k, n_seg = P.n_seg;
-  std::vector<double> amp((size_t)n_probes * n_seg), inten((size_t)n_probes * n_seg);
-  MSF_CUDA(cudaMemcpyAsync(amp.data(), P.amp.p, amp.size() * sizeof(double),
-                           cudaMemcpyDeviceToHost, stream));
-  MSF_CUDA(cudaMemcpyAsync(inten.data(), P.inten.p, inten.size() * sizeof(double),
-                           cudaMemcpyDeviceToHost, stream));
+  std::vector<double> amp((size_t)P.n_probes * P.n_seg), inten((size_t)P.n_probes * P.n_seg);
   std::vector<double> acc_a, acc_i;
   if (P.pix_modes) {
-    acc_a.resize(plane);
-    acc_i.resize(plane);
-    MSF_CUDA(cudaMemcpyAsync(acc_a.data(), P.acc_a.p, plane * sizeof(double),
-                             cudaMemcpyDeviceToHost, stream));
-    MSF_CUDA(cudaMemcpyAsync(acc_i.data(), P.acc_i.p, plane * sizeof(double),
-                             cudaMemcpyDeviceToHost, stream));
+    acc_a.resize(P.plane);
+    acc_i.resize(P.plane);
   }
-  MSF_CUDA(cudaStreamSynchronize(stream));
-  ctx->d2h_bytes += (int64_t)(2 * amp.size() * sizeof(double)) + (P.pix_modes ? 16 * plane : 0);
+  MSF_TRY(download_sums(ctx, P, stream, amp.data(), inten.data(),
+                        P.pix_modes ? acc_a.data() : nullptr,
+                        P.pix_modes ? acc_i.data() : nullptr));
+  return finish_host(P.spec->g, P.rings, P.optics, P.det, P.n_probes, amp.data(),
+                     inten.data(), P.pix_modes ? acc_a.data() : nullptr,
+                     P.pix_modes ? acc_i.data() : nullptr, res);
+}
 
-  if (P.want_adf && res->adf_image)
+msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& optics,
+                       const msf_detect& detect, int64_t n_probes, const double* amp,
+                       const double* inten, const double* acc_a, const double* acc_i,
+                       msf_results* res) {
+  const int64_t plane = (int64_t)g.nx * g.ny;
+  const uint32_t fem = detect.outputs & MSF_OUT_FEM_MASK;
+  const bool pix_modes = detect.outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE |
+                                           MSF_OUT_V_GT17 | MSF_OUT_V_RBAR);
+  const int n_k = fem ? rings.n_k : 0, n_seg = n_k + 1;
+  if (pix_modes && fem && (!acc_a || !acc_i)) {
+    set_error("pixel FEM modes need the per-pixel sums");
+    return MSF_ERR_ARG;
+  }
+  if ((detect.outputs & MSF_OUT_ADF_IMAGE) && res->adf_image)
     for (int64_t p = 0; p < n_probes; ++p) res->adf_image[p] = inten[p * n_seg + n_k];
 
   // ---- FEM statistics on the host, in the reference's order -----------
   res->n_k = n_k;
-  if (!P.fem) return MSF_OK;
+  if (!fem) return MSF_OK;
   if (n_k > res->cap_k) {
     set_error("results.cap_k is smaller than the number of k bins (" + std::to_string(n_k) + ")");
     return MSF_ERR_ARG;
   }
-  const Rings& rings = P.rings;
-  const msf_detect* det = &P.det;
+  const msf_detect* det = &detect;
   std::vector<uint8_t> inside(n_k);
   for (int k = 0; k < n_k; ++k)
-    inside[k] = (g.lambda * rings.bounds[k + 1] <= P.optics.alpha_max);  // adfstem.cpp:2518
+    inside[k] = (g.lambda * rings.bounds[k + 1] <= optics.alpha_max);  // adfstem.cpp:2518
   const std::vector<int32_t>& cnt = rings.counts;
   for (int k = 0; k < n_k; ++k) {
     if (res->k_lower) res->k_lower[k] = rings.bounds[k];
@@ -611,7 +652,7 @@ msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t str
       if (res->vbar_r && (det->outputs & MSF_OUT_VBAR_R)) res->vbar_r[k] = vs[k] / n_r;
     }
   }
-  if (P.pix_modes) {  // adfstem.cpp:2926-3612
+  if (pix_modes) {  // adfstem.cpp:2926-3612
     std::vector<double> mean_a(plane), mean_sq(plane), mean_i(plane), var(plane);
     for (int64_t p = 0; p < plane; ++p) {
       mean_a[p] = acc_a[p] / n_r;
@@ -643,7 +684,7 @@ msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t str
     }
     if (res->omega_vimage && (det->outputs & MSF_OUT_OMEGA_VIMAGE)) {
       const double lsq = g.lambda * g.lambda;
-      const double amax_sq = P.optics.alpha_max * P.optics.alpha_max;
+      const double amax_sq = optics.alpha_max * optics.alpha_max;
       for (int i = 0; i < g.nx; ++i)
         for (int j = 0; j < g.ny; ++j) {
           const int64_t p = j + (int64_t)g.ny * i;
@@ -659,11 +700,11 @@ msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t str
   return MSF_OK;
 }
 
-msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
-                      const msf_raster* raster, const msf_detect* det, msf_results* res) {
-  if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
-  RasterPlan P;
-  MSF_TRY(plan_raster(ctx, spec, optics, raster, det, &P));
+// The batched passes and detection over the plan's probes; the sums stay on
+// the device.  Fills the timing / count fields of `res` and, when asked,
+// final_psi (the plan's last probe).
+msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) {
+  const msf_specimen* spec = P.spec;
   const Grid& g = spec->g;
   const int64_t plane = P.plane, n_probes = P.n_probes;
   const bool fp64 = ctx->fp64;
@@ -843,7 +884,31 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
     res->kernel_launches =
         P.setup_launches + n_batches * (2 * S + 2 + (P.pix_modes ? 1 : 0));
   }
+  return MSF_OK;
+}
+
+msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                      const msf_raster* raster, const msf_detect* det, msf_results* res) {
+  if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
+  RasterPlan P;
+  MSF_TRY(plan_raster(ctx, spec, optics, raster, det, &P));
+  MSF_TRY(raster_sums(ctx, P, res));
   return finish_raster(ctx, P, ctx->stream, res);
+}
+
+msf_status run_partial(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                       const msf_raster* raster, const msf_detect* det, int64_t p_begin,
+                       int64_t p_end, double* amp, double* inten, double* acc_a,
+                       double* acc_i, msf_results* info) {
+  if (!spec || !optics || !raster || !det) { set_error("null argument"); return MSF_ERR_ARG; }
+  RasterPlan P;
+  MSF_TRY(plan_raster(ctx, spec, optics, raster, det, &P, p_begin, p_end));
+  msf_results local{};
+  msf_results* r = info ? info : &local;
+  r->final_psi = nullptr;
+  MSF_TRY(raster_sums(ctx, P, r));
+  r->n_k = P.n_k;
+  return download_sums(ctx, P, ctx->stream, amp, inten, acc_a, acc_i);
 }
 
 }  // namespace msf

@@ -82,6 +82,7 @@ struct RasterPlan {
   const msf_specimen* spec = nullptr;
   msf_optics optics{};
   msf_detect det{};
+  int64_t p_begin = 0, n_raster = 0;  // this plan's probes: [p_begin, p_begin + n_probes)
   int64_t n_probes = 0;
   int S = 0;
   int64_t plane = 0;
@@ -107,12 +108,30 @@ struct RasterPlan {
 // Device bytes plan_raster will allocate (for admission by an HBM budget).
 int64_t raster_plan_bytes(const msf_specimen* spec, bool fp64, int64_t n_probes,
                           bool pix_modes);
+// Plans probes [p_begin, p_end) of the raster (p_end < 0: to its end).
 msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
-                       const msf_raster* raster, const msf_detect* det, RasterPlan* plan);
+                       const msf_raster* raster, const msf_detect* det, RasterPlan* plan,
+                       int64_t p_begin = 0, int64_t p_end = -1);
+// Copies the plan's per-probe sums ([n_probes][n_seg] each) and pixel sums
+// to host arrays (any may be null), synchronising `stream`.
+msf_status download_sums(msf_context* ctx, const RasterPlan& P, cudaStream_t stream,
+                         double* amp, double* inten, double* acc_a, double* acc_i);
 // Copies the plan's sums to the host (synchronising `stream`) and finishes
 // the ADF image and FEM statistics in FP64 in the reference's order.
 msf_status finish_raster(msf_context* ctx, const RasterPlan& plan, cudaStream_t stream,
                          msf_results* res);
+// The ADF image and FEM statistics from per-probe sums of a whole raster
+// (host only): amp / inten [n_probes][n_k + 1] (ring sums, then the ADF
+// annulus), acc_a / acc_i the per-pixel sums over all probes (pixel modes).
+msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& optics,
+                       const msf_detect& detect, int64_t n_probes, const double* amp,
+                       const double* inten, const double* acc_a, const double* acc_i,
+                       msf_results* res);
+// Per-probe sums of probes [p_begin, p_end) of a raster (one shard).
+msf_status run_partial(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                       const msf_raster* raster, const msf_detect* det, int64_t p_begin,
+                       int64_t p_end, double* amp, double* inten, double* acc_a,
+                       double* acc_i, msf_results* info);
 
 msf_status build_specimen(msf_context* ctx, const msf_grid* grid, const msf_atoms* atoms,
                           msf_specimen* spec);

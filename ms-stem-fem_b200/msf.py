@@ -41,7 +41,8 @@ EXPORTED = [
     "msf_read_specimen", "msf_write_outputs", "msf_main", "msf_slice_atoms",
     "msf_time_passes", "msf_context_transfer_bytes", "msf_probe_noalloc",
     "msf_run_batch", "msf_server_create", "msf_server_submit", "msf_server_poll",
-    "msf_server_stats_get", "msf_server_destroy",
+    "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
+    "msf_finish",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -161,6 +162,13 @@ def lib() -> C.CDLL:
         L.msf_server_poll.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(Results)]
         L.msf_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         L.msf_server_destroy.argtypes = [C.c_void_p]
+        L.msf_segment_count.argtypes = [C.POINTER(Grid), C.POINTER(Detect)]
+        L.msf_segment_count.restype = C.c_int32
+        L.msf_run_partial.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics),
+                                      C.POINTER(Raster), C.POINTER(Detect), C.c_int64,
+                                      C.c_int64, _dp, _dp, _dp, _dp, C.POINTER(Results)]
+        L.msf_finish.argtypes = [C.POINTER(Grid), C.POINTER(Optics), C.POINTER(Detect),
+                                 C.c_int64, _dp, _dp, _dp, _dp, C.POINTER(Results)]
         L.msf_slice_atoms.argtypes = [C.c_int64, _dp, C.c_double, C.c_double, C.c_double,
                                       _ip, _dp, _dp, _lp, _lp, C.c_int32]
         L.msf_context_transfer_bytes.argtypes = [C.c_void_p, _lp, _lp, C.c_int32]
@@ -327,6 +335,26 @@ class Context:
             o.finish(j[2], j[3])
         return outs
 
+    def run_partial(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
+                    p_begin: int, p_end: int) -> dict:
+        """Per-probe sums of probes [p_begin, p_end) (msf_run_partial)."""
+        n_seg = segment_count(spec.grid, detect)
+        rows = max(p_end - p_begin, 0)  # the library rejects empty or reversed ranges
+        amp = np.zeros((rows, n_seg))
+        inten = np.zeros((rows, n_seg))
+        plane = spec.grid.nx * spec.grid.ny
+        pix = bool(detect.outputs & (OUT_V_RE | OUT_OMEGA_VIMAGE | OUT_V_GT17 | OUT_V_RBAR))
+        acc_a = np.zeros(plane) if pix else None
+        acc_i = np.zeros(plane) if pix else None
+        info = Results()
+        _check(lib().msf_run_partial(self._h, spec._h, C.byref(optics), C.byref(raster),
+                                     C.byref(detect), p_begin, p_end, _p(amp), _p(inten),
+                                     _p(acc_a) if pix else None, _p(acc_i) if pix else None,
+                                     C.byref(info)))
+        return {"amp": amp, "inten": inten, "acc_a": acc_a, "acc_i": acc_i,
+                "probe_slices": info.probe_slices, "kernel_launches": info.kernel_launches,
+                "seconds_raster": info.seconds_raster, "n_k": info.n_k}
+
     def time_passes(self, spec: "Specimen", nb: int, reps: int = 10):
         """Mean ms per launch of the fused row and column slice passes."""
         r, c = C.c_double(), C.c_double()
@@ -337,6 +365,29 @@ class Context:
         out = np.zeros(2 * spec.grid.nx * spec.grid.ny)
         _check(lib().msf_probe(self._h, spec._h, C.byref(optics), _p(out)))
         return out.reshape(spec.grid.nx, spec.grid.ny, 2)
+
+
+def segment_count(grid: Grid, detect: Detect) -> int:
+    """Detector segments per probe: FEM ring bins, then the ADF annulus."""
+    return lib().msf_segment_count(C.byref(grid), C.byref(detect))
+
+
+def finish(grid: Grid, optics: Optics, raster: Raster, detect: Detect, amp, inten,
+           acc_a=None, acc_i=None, want_means=False, cap_k=8192) -> "RunResult":
+    """ADF image and FEM statistics from the per-probe rows of a whole raster
+    (msf_finish; host only, no GPU)."""
+    amp = np.ascontiguousarray(amp, dtype=np.float64)
+    inten = np.ascontiguousarray(inten, dtype=np.float64)
+    n = raster.n_x * raster.n_y
+    assert amp.shape[0] == n and inten.shape[0] == n
+    out = RunResult(n, cap_k, grid.nx, grid.ny, False, want_means)
+    a_a = None if acc_a is None else np.ascontiguousarray(acc_a, dtype=np.float64)
+    a_i = None if acc_i is None else np.ascontiguousarray(acc_i, dtype=np.float64)
+    _check(lib().msf_finish(C.byref(grid), C.byref(optics), C.byref(detect), n, _p(amp),
+                            _p(inten), None if a_a is None else _p(a_a),
+                            None if a_i is None else _p(a_i), C.byref(out._struct)))
+    out.finish(raster, detect)
+    return out
 
 
 class Server:
