@@ -81,17 +81,21 @@ def ncu_traffic(which, name="row_col_pass_1024_fp32.md"):
 def plain_and_precision(msf, job, q, z, device, argv_sample, res32):
     """The two comparisons the headline metric is quoted with.
 
-    plain: probe*slices/s of the plain GPU path - FP64 wavefields, one probe
-    per launch, no CUDA graph, same specimen - on an 8x8 raster sample.
+    plain: probe*slices/s of the plain GPU path (msf_run_plain: FP64
+    wavefields, one probe at a time, one launch per step of the reference's
+    slice loop, no CUDA graph) on an 8x8 raster sample of the same specimen;
+    fused_1: the fused FP64 passes with one probe per launch, same sample.
     v_err: per FEM mode, the largest relative deviation over the k bins of
     the FP32 run's V(k) from an FP64 GPU run of the full workload (bins with
     |V| <= 1e-6 excluded)."""
     jp = msf.Job(argv_sample)
     cp = msf.Context(device=device, precision="fp64", batch=1, graphs=False)
     sp = cp.specimen(jp.grid, q, z)
-    cp.run(sp, jp.optics, jp.raster, jp.detect)
-    rp = cp.run(sp, jp.optics, jp.raster, jp.detect)
+    cp.run_plain(sp, jp.optics, jp.raster, jp.detect)
+    rp = cp.run_plain(sp, jp.optics, jp.raster, jp.detect)
     plain = rp.probe_slices / rp.seconds_raster
+    rf = cp.run(sp, jp.optics, jp.raster, jp.detect)
+    fused_1 = rf.probe_slices / rf.seconds_raster
     sp.close()
     cp.close()
     c64 = msf.Context(device=device, precision="fp64")
@@ -105,7 +109,7 @@ def plain_and_precision(msf, job, q, z, device, argv_sample, res32):
     fp64_rate = r64.probe_slices / r64.seconds_raster
     s64.close()
     c64.close()
-    return plain, errs, fp64_rate
+    return plain, fused_1, errs, fp64_rate
 
 
 class ClockSampler:
@@ -235,6 +239,214 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- configs
+def _grid(msf, n, box, zbox, voltage=200000.0):
+    return msf.Grid(nx=n, ny=n, voltage=voltage, xperiod=box, yperiod=box, zperiod=zbox,
+                    dupe_x=1, dupe_y=1, dupe_z=1, replicate_atoms=0, xmin=0.0, ymin=0.0,
+                    zmin=0.0, min_slice=2.0)
+
+
+class Raster:
+    """n x n probes at i * box / n (func.cpp:108-127), arrays kept alive."""
+
+    def __init__(self, msf, n, box):
+        self.xp = np.arange(n) * (box / n)
+        self.r = msf.Raster(n, n, self.xp.ctypes.data_as(msf._dp),
+                            self.xp.ctypes.data_as(msf._dp))
+
+
+def fem_optics(msf):
+    return msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0, defocus=0.0, alpha_max=0.0015)
+
+
+def adf_optics(msf, voltage=200000.0):
+    lam = msf.wavelength(voltage)[0]
+    return msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0,
+                      defocus=msf.lib().msf_scherzer(0, lam, 1.3e7), alpha_max=0.010)
+
+
+def batch_specimens(msf):
+    """Eight seeded amorphous-Si cubes, edges 50..200 A, grids 512^2..2048^2
+    at ~0.1 A sampling, 50 atoms/nm^3, 32x32 rasters."""
+    grids = [512, 512, 1024, 1024, 1024, 2048, 2048, 2048]
+    out = []
+    for s, n in enumerate(grids):
+        edge = 50.0 + 150.0 * s / 7
+        q = msf.amorphous_positions(int(round(0.05 * edge ** 3)), (edge, edge, edge), 2.2,
+                                    seed=31 + s)
+        out.append((n, edge, q))
+    return out
+
+
+def workload_batch(args, msf, local):
+    """8 uneven specimens in slot lanes (one per grid size) against the same
+    rasters run one after another with msf_run."""
+    ctx = msf.Context(device=local, precision="fp32")
+    det = msf.Detect(outputs=msf.OUT_ADF_IMAGE | msf.OUT_V_OMEGA, det_inner=0.04,
+                     det_outer=0.2, dr=1.2065)
+    jobs, keep = [], []
+    t0 = time.time()
+    for n, edge, q in batch_specimens(msf):
+        spec = ctx.specimen(_grid(msf, n, edge, edge), q, np.full(len(q), 14, np.uint32))
+        r = Raster(msf, 32, edge)
+        keep.append(r)
+        jobs.append((spec, fem_optics(msf), r.r, det))
+    setup = time.time() - t0
+    for _ in range(max(1, args.warmup)):
+        ctx.run_batch(jobs, slots=args.batch)
+    times, ps = [], 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            outs = ctx.run_batch(jobs, slots=args.batch)
+            times.append(max(o.seconds_raster for o in outs))
+            ps = sum(o.probe_slices for o in outs)
+            launches = max(o.kernel_launches for o in outs)
+    seq = 0.0
+    for spec, o, r, d in jobs:
+        seq += ctx.run(spec, o, r, d).seconds_raster
+    t = statistics.median(times)
+    line = {"metric": "probe*slice props/s, 8 uneven specimens 512^2-2048^2 in slot lanes",
+            "value": round(ps / t, 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * t, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "8 amorphous-Si cubes 50..200 A, grids 512,512,1024x3,"
+                                   "2048x3, 32x32 rasters, 2 A slices, V_omega + ADF",
+                       "probe_slices_per_step": ps,
+                       "slots_per_lane": args.batch or "auto: ~2 GiB of wavefields per lane",
+                       "specimen_setup_s": round(setup, 2)},
+            "sequential_msf_run": {"value": round(ps / seq, 1), "unit": UNIT},
+            "clocks": clocks.summary(), "gpu_launches": int(launches)}
+    print(json.dumps(line))
+    return 0
+
+
+def workload_stress(args, msf, local):
+    """600k atoms, 200x200x300 A, 2048^2, 300 kV, 150 slices, 16x16 raster:
+    FP32 split-wave against FP64 wavefields, per-output error."""
+    box = (200.0, 200.0, 300.0)
+    q = msf.amorphous_positions(600000, box, 2.2, seed=4)
+    z = np.full(len(q), 14, np.uint32)
+    lam = msf.wavelength(300000.0)[0]
+    optics = msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0,
+                        defocus=msf.lib().msf_scherzer(0, lam, 1.3e7),
+                        alpha_max=msf.lib().msf_scherzer(1, lam, 1.3e7))
+    det = msf.Detect(outputs=msf.OUT_ADF_IMAGE | msf.OUT_V_OMEGA, det_inner=0.04,
+                     det_outer=0.2, dr=1.0)
+    r = Raster(msf, 16, box[0])
+    out = {}
+    for prec in ("fp32", "fp64"):
+        ctx = msf.Context(device=local, precision=prec)
+        t0 = time.time()
+        spec = ctx.specimen(_grid(msf, 2048, box[0], box[2], voltage=300000.0), q, z)
+        setup = time.time() - t0
+        ctx.run(spec, optics, r.r, det)
+        res = ctx.run(spec, optics, r.r, det)
+        out[prec] = (res, setup, spec.slices()["n"])
+        spec.close()
+        ctx.close()
+    r32, r64 = out["fp32"][0], out["fp64"][0]
+    adf_err = float(np.max(np.abs(r32.adf_image - r64.adf_image) / np.abs(r64.adf_image)))
+    v64 = r64.v["V_omega"]
+    ok = np.isfinite(v64) & (np.abs(v64) > 1e-6)
+    v_err = float(np.max(np.abs(r32.v["V_omega"][ok] - v64[ok]) / np.abs(v64[ok])))
+    line = {"metric": "probe*slice props/s @2048^2, 150 slices, 300 kV (FP32 split-wave)",
+            "value": round(r32.probe_slices / r32.seconds_raster, 1), "unit": UNIT,
+            "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": round(1e3 * r32.seconds_raster, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "600k Si atoms 200x200x300 A, 2048^2, 300 kV, Scherzer, "
+                                   "16x16 raster", "slices": out["fp32"][2],
+                       "specimen_setup_s": round(out["fp32"][1], 2)},
+            "fp64": {"value": round(r64.probe_slices / r64.seconds_raster, 1), "unit": UNIT,
+                     "specimen_setup_s": round(out["fp64"][1], 2)},
+            "error_fp32_vs_fp64": {"adf_image_max_rel": adf_err, "v_omega_max_rel": v_err},
+            "gpu_launches": int(r32.kernel_launches)}
+    print(json.dumps(line))
+    return 0
+
+
+def serving_requests(msf, n_jobs, seed=5):
+    """Seeded request stream: grid from {256,512,1024,2048}^2 at 0.09766 A
+    sampling, raster 8..64 per side, thickness 50..300 A, ADF or FEM V(k)
+    with probability 1/2, 50 atoms/nm^3 per request."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n_jobs):
+        n = int(rng.choice([256, 512, 1024, 2048]))
+        edge = n * 0.09766
+        n_r = int(rng.integers(8, 65))
+        thick = float(rng.uniform(50.0, 300.0))
+        fem = bool(rng.random() < 0.5)
+        q = msf.amorphous_positions(int(round(0.05 * edge * edge * thick)), (edge, edge, thick),
+                                    2.2, seed=5000 + k)
+        det = (msf.Detect(outputs=msf.OUT_V_OMEGA, det_inner=0.04, det_outer=0.2, dr=1.0)
+               if fem else
+               msf.Detect(outputs=msf.OUT_ADF_IMAGE, det_inner=0.04, det_outer=0.2, dr=1.0))
+        reqs.append({"grid": _grid(msf, n, edge, thick), "q": q,
+                     "z": np.full(len(q), 14, np.uint32),
+                     "optics": fem_optics(msf) if fem else adf_optics(msf),
+                     "raster": Raster(msf, n_r, edge), "detect": det, "n": n, "fem": fem})
+    return reqs
+
+
+def run_serving(msf, local, n_jobs, rate, slots, seed=5):
+    """Poisson arrivals at `rate` jobs/s into msf_server; returns the summary."""
+    reqs = serving_requests(msf, n_jobs, seed)
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, n_jobs)
+    srv = msf.Server(device=local, slots=slots)
+    # warm-up: one small request per grid size (lanes, graphs, module load)
+    warm = []
+    for n in (256, 512, 1024, 2048):
+        edge = n * 0.09766
+        q = msf.amorphous_positions(int(0.05 * edge * edge * 6), (edge, edge, 6.0), 2.2, seed=n)
+        r = Raster(msf, 2, edge)
+        warm.append((srv.submit(_grid(msf, n, edge, 6.0), q, np.full(len(q), 14, np.uint32),
+                                fem_optics(msf), r.r,
+                                msf.Detect(outputs=msf.OUT_V_OMEGA, det_inner=0.04,
+                                           det_outer=0.2, dr=1.0)), r))
+    for t, _ in warm:
+        while srv.poll(t, wait_ms=100) is None:
+            pass
+    srv.close()
+    srv = msf.Server(device=local, slots=slots)
+    tickets = []
+    t_start = time.time()
+    t_next = t_start
+    for req, gap in zip(reqs, gaps):
+        t_next += gap
+        dt = t_next - time.time()
+        if dt > 0:
+            time.sleep(dt)
+        tickets.append(srv.submit(req["grid"], req["q"], req["z"], req["optics"],
+                                  req["raster"].r, req["detect"]))
+    for t in tickets:
+        while srv.poll(t, wait_ms=200) is None:
+            pass
+    st = srv.stats()
+    wall = time.time() - t_start
+    srv.close()
+    return {"jobs": n_jobs, "arrival_rate_per_s": rate, "slots_per_lane": slots,
+            "p50_s": round(st["p50_s"], 3), "p99_s": round(st["p99_s"], 3),
+            "max_s": round(st["max_s"], 3), "completed": st["completed"],
+            "failed": st["failed"], "probe_slices": st["probe_slices"],
+            "throughput": round(st["probe_slices"] / wall, 1), "unit": UNIT,
+            "wall_s": round(wall, 2),
+            "mix": {str(n): sum(1 for r in reqs if r["n"] == n) for n in (256, 512, 1024, 2048)}}
+
+
+def workload_serving(args, msf, local):
+    s = run_serving(msf, local, args.jobs, args.rate, args.batch)
+    line = {"metric": "serving p99 latency, Poisson arrivals, mixed 256^2-2048^2 requests",
+            "value": s["p99_s"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": None, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "request stream: grids 256..2048^2, rasters 8..64^2, "
+                                   "5..30 nm thick, ADF or FEM, 50 atoms/nm^3"},
+            "serving": s}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,11 +463,26 @@ def main():
     ap.add_argument("--raster", type=int, default=0,
                     help="probes per raster side (default 64, the workload's); smaller "
                          "values make a short case for profiling")
+    ap.add_argument("--workload", default="fem",
+                    choices=["fem", "batch", "stress", "serving"],
+                    help="fem: the headline FEM raster (default); batch: 8 uneven specimens "
+                         "in slot lanes; stress: 2048^2, 150 slices, FP32 vs FP64; serving: "
+                         "Poisson request stream through msf_server")
+    ap.add_argument("--jobs", type=int, default=24, help="requests of --workload serving")
+    ap.add_argument("--rate", type=float, default=20.0, help="request arrivals per second")
+    ap.add_argument("--serving-jobs", type=int, default=8,
+                    help="requests of the serving sample in the headline line (0: none)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
 
     import msf
+    if args.workload != "fem":
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        return {"batch": workload_batch, "stress": workload_stress,
+                "serving": workload_serving}[args.workload](args, msf, local)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -392,13 +619,21 @@ def main():
     if world == 1 and not args.no_plain and args.precision == "fp32":
         sample = list(argv)
         sample[sample.index("--rasterspacing") + 1] = repr(WORKLOAD["box"][0] / 8)
-        plain, v_err, fp64_rate = plain_and_precision(msf, job, q, z, local, sample, last)
+        plain, fused_1, v_err, fp64_rate = plain_and_precision(msf, job, q, z, local, sample,
+                                                               last)
         versus = {"plain_gpu": {"value": round(plain, 1), "unit": UNIT,
-                                "path": "FP64 wavefields, 1 probe per launch, no CUDA graph",
+                                "path": "msf_run_plain: FP64, one probe at a time, one launch "
+                                        "per reference step, no CUDA graph",
                                 "sample": "8x8 raster of the same specimen"},
                   "batched_vs_plain": round(value / plain, 2),
+                  "fused_fp64_one_probe": {"value": round(fused_1, 1), "unit": UNIT},
+                  "batched_vs_fused_one_probe": round(value / fused_1, 2),
                   "fp64_batched": {"value": round(fp64_rate, 1), "unit": UNIT},
                   "v_err_vs_fp64": v_err, "v_err_bound": 1e-4}
+
+    serving = None
+    if world == 1 and args.serving_jobs > 0:
+        serving = run_serving(msf, local, args.serving_jobs, args.rate, 0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -425,6 +660,7 @@ def main():
                            "graphs": not args.no_graphs, "batch": args.batch or "auto",
                            "specimen_setup_s": round(setup_s, 3)},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "versus": versus,
+                "serving": serving,
                 "clocks": clocks.summary(), "gpu_launches": int(launches),
                 "wall_s_timed": round(wall, 3)}
         print(json.dumps(line))

@@ -168,6 +168,14 @@ int64_t msf_specimen_device_bytes(const msf_specimen* spec);
 msf_status msf_run(msf_context* ctx, const msf_specimen* spec,
                    const msf_optics* optics, const msf_raster* raster,
                    const msf_detect* detect, msf_results* results);
+/* The same raster as msf_run, computed the plain way: one probe at a time,
+ * FP64, one kernel launch per step of the reference's loop
+ * (adfstem.cpp:1632-2132: place probe, FFT, / sqrt(NxNy); per slice iFFT,
+ * transmission, FFT, / sqrt(NxNy), bw_limit, propagate), no graph.  The
+ * comparator the batched path is measured against; FP64 contexts only. */
+msf_status msf_run_plain(msf_context* ctx, const msf_specimen* spec,
+                         const msf_optics* optics, const msf_raster* raster,
+                         const msf_detect* detect, msf_results* results);
 /* Normalised real-space probe (adfstem.cpp:586-817), 2*nx*ny doubles. */
 msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
                      const msf_optics* optics, double* out);
@@ -217,8 +225,9 @@ msf_status msf_finish(const msf_grid* grid, const msf_optics* optics,
 /* Several rasters at once: results[i] is what msf_run(ctx, specs[i],
  * &optics[i], &rasters[i], &detects[i], &results[i]) returns, within FP32
  * rounding (final_psi is not filled).  Rasters of the same grid size share
- * launches: each of `slots` wavefields (0: up to 256, bounded by free
- * memory) carries one probe of any raster at its own slice, and a slot whose
+ * launches: each of `slots` wavefields (0: about 2 GiB of wavefields,
+ * 16..256, bounded by free memory) carries one probe of any raster at its
+ * own slice, and a slot whose
  * probe finished is refilled with the next waiting probe.  Grid sizes run as
  * separate lanes on separate streams that overlap on the GPU.  FP32 contexts
  * only.  results[i].seconds_raster is the device time from the start of the
@@ -251,8 +260,8 @@ typedef struct msf_server msf_server;
  * requests in arrival order while their estimated device bytes fit
  * `opt->hbm_budget` (0: 80 % of free memory), builds each specimen, and
  * feeds its probes into the slot lane of its grid size (`slots` wavefields
- * per lane, 0: 64); requests that arrive while others run join the running
- * launches as slots free up. */
+ * per lane; 0: about 2 GiB of wavefields, 16..256, by grid size); requests
+ * that arrive while others run join the running launches as slots free up. */
 msf_status msf_server_create(const msf_options* opt, int32_t slots, msf_server** out);
 /* Queue a request; returns at once with its ticket. */
 msf_status msf_server_submit(msf_server* srv, const msf_request* req, uint64_t* ticket);
@@ -289,6 +298,15 @@ msf_status msf_slice_atoms(int64_t n_atoms, const double* q, double zmin,
                            double zperiod, double min_slice, int32_t* n_slices,
                            double* lower, double* thickness, int64_t* counts,
                            int64_t* order, int32_t cap);
+
+/* ---- specimen generator (no counterpart in the reference) -------------- */
+/* Seeded amorphous positions: random sequential addition of n_atoms points
+ * uniform in [0, box[0]) x [0, box[1]) x [0, box[2]) with a minimum periodic
+ * separation min_sep [A]; proposals from std::mt19937_64(seed) mapped to
+ * doubles as (x >> 11) * 2^-53.  q receives 3*n_atoms coordinates.  Fails
+ * with MSF_ERR_ARG when max_proposals (0: 1000 per atom) run out first. */
+msf_status msf_amorphous_positions(int64_t n_atoms, const double* box, double min_sep,
+                                   uint64_t seed, int64_t max_proposals, double* q);
 
 /* ---- measurement hook (no counterpart in the reference) ---------------- */
 /* Time the two fused slice passes on a resident batch of `nb` wavefields:

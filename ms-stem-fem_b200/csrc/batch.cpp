@@ -1,5 +1,7 @@
 // msf_run_batch: several rasters through slot lanes, one lane per grid size.
 #include <algorithm>
+#include <chrono>
+#include <thread>
 #include <map>
 #include <memory>
 #include <string>
@@ -30,14 +32,17 @@ namespace {
 
 }  // namespace
 
-// Slots of a lane: `want`, or up to 256 bounded by half the free memory
-// shared among `lanes` lanes.
+// Slots of a lane: `want`, or about 2 GiB of FP32 wavefields, clamped to
+// [16, 256] (measured on B200: 256 slots at 512^2 and 1024^2, 64 at 2048^2;
+// larger sets of wavefields run slower), bounded by the lane's probes and by
+// half the free memory shared among `lanes` lanes.
 int lane_slots(int want, int64_t plane, int lanes, int64_t probes) {
   if (want > 0) return want;
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const int64_t cap = (int64_t)(0.5 * (double)free_b / std::max(1, lanes)) / (8 * plane);
-  return (int)std::max<int64_t>(1, std::min<int64_t>({cap, 256, probes}));
+  const int64_t footprint = std::max<int64_t>(16, std::min<int64_t>(256, (2LL << 30) / (8 * plane)));
+  return (int)std::max<int64_t>(1, std::min<int64_t>({cap, footprint, probes}));
 }
 
 msf_status run_batch(msf_context* ctx, int n, const msf_specimen* const* specs,
@@ -92,13 +97,19 @@ msf_status run_batch(msf_context* ctx, int n, const msf_specimen* const* specs,
   msf_status st = MSF_OK;
   bool any = true;
   while (any && st == MSF_OK) {
+    // step every lane that can take a step without waiting, so that a lane
+    // of small grids is not paced by one of large grids
     any = false;
+    bool stepped = false;
     for (auto& lane : lanes) {
       if (!lane->busy()) continue;
       any = true;
+      if (!lane->ready()) continue;
       st = lane->step();
+      stepped = true;
       if (st != MSF_OK) break;
     }
+    if (any && !stepped) std::this_thread::sleep_for(std::chrono::microseconds(20));
     for (int i = 0; i < n && st == MSF_OK; ++i)
       if (jobs[i]->complete && !stamped[i]) {
         cudaError_t e = cudaEventRecord(stop[i], lanes[lane_of[i]]->stream());

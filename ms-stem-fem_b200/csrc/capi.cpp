@@ -193,6 +193,16 @@ msf_status msf_run(msf_context* ctx, const msf_specimen* spec, const msf_optics*
   return run_raster(ctx, spec, optics, raster, detect, results);
 }
 
+msf_status msf_run_plain(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
+                         const msf_raster* raster, const msf_detect* detect,
+                         msf_results* results) {
+  if (!ctx || !spec || spec->ctx != ctx) {
+    set_error("specimen does not belong to this context");
+    return MSF_ERR_ARG;
+  }
+  return run_raster_plain(ctx, spec, optics, raster, detect, results);
+}
+
 int32_t msf_segment_count(const msf_grid* grid, const msf_detect* detect) {
   if (!grid || !detect) return -1;
   if (!(detect->outputs & MSF_OUT_FEM_MASK)) return 1;

@@ -896,6 +896,101 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
   return finish_raster(ctx, P, ctx->stream, res);
 }
 
+msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
+                            const msf_optics* optics, const msf_raster* raster,
+                            const msf_detect* det, msf_results* res) {
+  if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
+  if (!ctx->fp64) {
+    set_error("the plain per-pass path runs FP64 wavefields: use an MSF_FP64 context");
+    return MSF_ERR_UNSUPPORTED;
+  }
+  RasterPlan P;
+  MSF_TRY(plan_raster(ctx, spec, optics, raster, det, &P));
+  const Grid& g = spec->g;
+  const int64_t plane = P.plane;
+  const int S = P.S;
+  cudaStream_t st = ctx->stream;
+  DevBuf psi, d_partial;
+  MSF_TRY(ctx->alloc(&psi, 16 * plane));
+  MSF_TRY(ctx->alloc(&d_partial, sizeof(double) * 2 * std::max(P.n_chunks, 1)));
+  SegmentPlan seg;
+  seg.idx = P.seg_idx.as<int32_t>();
+  seg.chunk_begin = P.chunk_begin.as<int32_t>();
+  seg.seg_chunk = P.seg_chunk.as<int32_t>();
+  seg.n_chunks = P.n_chunks;
+  seg.ng = P.n_seg;
+  seg.partial = d_partial.as<double>();
+  PassArgs a;
+  a.psi = psi.p;
+  a.batch_stride = plane;
+  a.nb = 1;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  a.scale = 1.0;
+  const void *tw_y = nullptr, *tw_x = nullptr;
+  MSF_TRY(ctx->twiddles(g.ny, true, &tw_y));
+  MSF_TRY(ctx->twiddles(g.nx, true, &tw_x));
+  auto fft2 = [&](bool inverse) -> msf_status {
+    a.tw = tw_y;
+    MSF_CUDA(launch_row(true, inverse ? ROW_INV : ROW_FWD, a, st));
+    a.tw = tw_x;
+    MSF_CUDA(launch_col(true, inverse ? COL_INV : COL_FWD, a, st));
+    return MSF_OK;
+  };
+  const double* t0 = spec->t.as<double>();
+  const double* prop = spec->prop.as<double>();
+  const int32_t* lo = spec->mask_lo.as<int32_t>();
+  const int32_t* hi = spec->mask_hi.as<int32_t>();
+  double* d = psi.as<double>();
+  cudaEvent_t ev0, ev1;
+  MSF_CUDA(cudaEventCreate(&ev0));
+  MSF_CUDA(cudaEventCreate(&ev1));
+  MSF_CUDA(cudaEventRecord(ev0, st));
+  int64_t launches = 0;
+  for (int64_t p = 0; p < P.n_probes; ++p) {
+    // a15-a16: shifted probe, FORWARD transform, / sqrt(NxNy)
+    MSF_CUDA(launch_place_probe(d, P.probe64.as<double>(), g.nx, g.ny, P.shifts[2 * p],
+                                P.shifts[2 * p + 1], st));
+    MSF_TRY(fft2(false));
+    MSF_CUDA(launch_scale(d, plane, 1.0 / g.s, nullptr, st));
+    launches += 4;
+    for (int s = 0; s < S; ++s) {  // a17, one reference step per launch
+      MSF_TRY(fft2(true));
+      MSF_CUDA(launch_transmit(d, t0 + 2 * plane * s, plane, 1.0 / g.s, st));
+      MSF_TRY(fft2(false));
+      MSF_CUDA(launch_scale(d, plane, 1.0 / g.s, nullptr, st));
+      MSF_CUDA(launch_bw_limit(d, lo, hi, g.nx, g.ny, st));
+      const double* px = prop + 2 * (size_t)(g.nx + g.ny) * s;
+      MSF_CUDA(launch_propagate(d, px, px + 2 * g.nx, lo, hi, g.nx, g.ny, st));
+      launches += 8;
+    }
+    SplitK none;
+    MSF_CUDA(launch_segment_sums(true, d, plane, 1, seg, P.amp.as<double>() + p * P.n_seg,
+                                 P.inten.as<double>() + p * P.n_seg, none, st));
+    launches += 2;
+    if (P.pix_modes) {
+      MSF_CUDA(launch_pixel_accum(true, d, plane, 1, plane, P.acc_a.as<double>(),
+                                  P.acc_i.as<double>(), none, st));
+      launches += 1;
+    }
+  }
+  MSF_CUDA(cudaEventRecord(ev1, st));
+  MSF_CUDA(cudaEventSynchronize(ev1));
+  float ms = 0;
+  MSF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  res->seconds_raster = 1e-3 * ms;
+  res->seconds_setup = 0;
+  res->probe_slices = P.n_probes * S;
+  res->kernel_launches = P.setup_launches + launches;
+  if (res->final_psi) {
+    MSF_CUDA(cudaMemcpy(res->final_psi, d, 16 * plane, cudaMemcpyDeviceToHost));
+    ctx->d2h_bytes += 16 * plane;
+  }
+  return finish_raster(ctx, P, st, res);
+}
+
 msf_status run_partial(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                        const msf_raster* raster, const msf_detect* det, int64_t p_begin,
                        int64_t p_end, double* amp, double* inten, double* acc_a,

@@ -127,6 +127,10 @@ msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& opti
                        const msf_detect& detect, int64_t n_probes, const double* amp,
                        const double* inten, const double* acc_a, const double* acc_i,
                        msf_results* res);
+// The raster one probe at a time, one launch per reference step (FP64).
+msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
+                            const msf_optics* optics, const msf_raster* raster,
+                            const msf_detect* det, msf_results* res);
 // Per-probe sums of probes [p_begin, p_end) of a raster (one shard).
 msf_status run_partial(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                        const msf_raster* raster, const msf_detect* det, int64_t p_begin,

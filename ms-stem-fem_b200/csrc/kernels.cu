@@ -686,6 +686,55 @@ __global__ void assemble_split_kernel(const float2* __restrict__ delta, SplitK s
   out[p] = exit_value<float>(delta, (int)p, sk, sx, sy);
 }
 
+// ---- plain per-pass path (FP64, one probe): one kernel per reference step
+// psi[i][j] = probe[(i - sx) mod nx][(j - sy) mod ny] (adfstem.cpp:1632-1671)
+__global__ void place_probe_kernel(double2* __restrict__ psi, const double2* __restrict__ probe,
+                                   int nx, int ny, int sx, int sy) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)nx * ny) return;
+  const int i = (int)(k / ny), j = (int)(k - (int64_t)i * ny);
+  const int ii = i < sx ? i + nx - sx : i - sx;
+  const int jj = j < sy ? j + ny - sy : j - sy;
+  psi[k] = probe[(int64_t)ii * ny + jj];
+}
+
+// psi <- t * psi / s with the reference's in-place update order: the new
+// real part feeds the imaginary part (adfstem.cpp:1929-1949)
+__global__ void transmit_kernel(double2* __restrict__ psi, const double2* __restrict__ t,
+                                int64_t n, double inv_s) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double2 v = psi[k], tv = t[k];
+  const double re = (tv.x * v.x - tv.y * v.y) * inv_s;
+  const double im = (tv.x * v.y + tv.y * re) * inv_s;
+  psi[k] = make_double2(re, im);
+}
+
+// zero outside the band limit (bw_limit.cpp:30-47): column j keeps rows
+// i < lo[j] and i >= hi[j]
+__global__ void bw_limit_kernel(double2* __restrict__ psi, const int32_t* __restrict__ lo,
+                                const int32_t* __restrict__ hi, int nx, int ny) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)nx * ny) return;
+  const int i = (int)(k / ny), j = (int)(k - (int64_t)i * ny);
+  if (!(i < lo[j] || i >= hi[j])) psi[k] = make_double2(0.0, 0.0);
+}
+
+// psi(k) <- P_x(kx) P_y(ky) psi(k) inside the band limit, else 0
+// (slice.cpp:1366-1421)
+__global__ void propagate_kernel(double2* __restrict__ psi, const double2* __restrict__ px,
+                                 const double2* __restrict__ py, const int32_t* __restrict__ lo,
+                                 const int32_t* __restrict__ hi, int nx, int ny) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)nx * ny) return;
+  const int i = (int)(k / ny), j = (int)(k - (int64_t)i * ny);
+  if (i < lo[j] || i >= hi[j]) {
+    psi[k] = cmul(cmul(px[i], py[j]), psi[k]);
+  } else {
+    psi[k] = make_double2(0.0, 0.0);
+  }
+}
+
 inline unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
 
 }  // namespace
@@ -812,6 +861,35 @@ cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t stride, int 
     if (e != cudaSuccess) return e;
   }
   segment_reduce_kernel<<<nb, 128, 0, s>>>(pa, pi, sp.seg_chunk, sp.ng, sp.n_chunks, amp, inten);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_place_probe(double* psi, const double* probe, int nx, int ny, int sx, int sy,
+                               cudaStream_t s) {
+  place_probe_kernel<<<blocks_for((int64_t)nx * ny, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(psi), reinterpret_cast<const double2*>(probe), nx, ny, sx, sy);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transmit(double* psi, const double* t, int64_t n, double inv_s,
+                            cudaStream_t s) {
+  transmit_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(psi), reinterpret_cast<const double2*>(t), n, inv_s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bw_limit(double* psi, const int32_t* lo, const int32_t* hi, int nx, int ny,
+                            cudaStream_t s) {
+  bw_limit_kernel<<<blocks_for((int64_t)nx * ny, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(psi), lo, hi, nx, ny);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_propagate(double* psi, const double* px, const double* py, const int32_t* lo,
+                             const int32_t* hi, int nx, int ny, cudaStream_t s) {
+  propagate_kernel<<<blocks_for((int64_t)nx * ny, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(psi), reinterpret_cast<const double2*>(px),
+      reinterpret_cast<const double2*>(py), lo, hi, nx, ny);
   return cudaGetLastError();
 }
 

@@ -183,6 +183,16 @@ struct DetectTable {
 cudaError_t launch_slot_detect(const void* table, int max_done, int max_chunks, int nx, int ny,
                                double* partial, bool pixel_sums, cudaStream_t s);
 
+// ---- plain per-pass path (FP64, one probe, one kernel per reference step)
+cudaError_t launch_place_probe(double* psi, const double* probe, int nx, int ny, int sx, int sy,
+                               cudaStream_t s);
+cudaError_t launch_transmit(double* psi, const double* t, int64_t n, double inv_s,
+                            cudaStream_t s);
+cudaError_t launch_bw_limit(double* psi, const int32_t* lo, const int32_t* hi, int nx, int ny,
+                            cudaStream_t s);
+cudaError_t launch_propagate(double* psi, const double* px, const double* py, const int32_t* lo,
+                             const int32_t* hi, int nx, int ny, cudaStream_t s);
+
 // acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
                                int nb, int64_t npix, double* acc_a, double* acc_i,

@@ -33,7 +33,8 @@ Lane::Lane(msf_context* ctx, int nx, int ny, int slots)
 
 Lane::~Lane() {
   if (stream_) cudaStreamSynchronize(stream_);
-  if (graph_) cudaGraphExecDestroy(graph_);
+  if (graph_pass_) cudaGraphExecDestroy(graph_pass_);
+  if (graph_detect_) cudaGraphExecDestroy(graph_detect_);
   for (auto& e : ring_ev_)
     if (e) cudaEventDestroy(e);
   if (host_ring_) cudaFreeHost(host_ring_);
@@ -83,9 +84,9 @@ msf_status Lane::init() {
 
 msf_status Lane::grow_chunks(int n_chunks) {
   MSF_CUDA(cudaStreamSynchronize(stream_));
-  if (graph_) {
-    cudaGraphExecDestroy(graph_);
-    graph_ = nullptr;
+  if (graph_detect_) {  // it holds the old scratch pointer
+    cudaGraphExecDestroy(graph_detect_);
+    graph_detect_ = nullptr;
   }
   max_chunks_ = std::max(n_chunks, 1);
   MSF_TRY(ctx_->alloc(&partial_, sizeof(double) * 2 * (size_t)B_ * max_chunks_));
@@ -108,28 +109,43 @@ msf_status Lane::add(SlotJob* job) {
   return MSF_OK;
 }
 
-msf_status Lane::launch_step() {
+msf_status Lane::launch_passes() {
   MSF_CUDA(launch_row(false, ROW_SLOTS, row_, stream_));
   if (pipe_col_)
     MSF_CUDA(launch_col_slice_pipe(col_, false, col_map_, err_.as<int>(), stream_));
   else
     MSF_CUDA(launch_col(false, COL_SLOTS, col_, stream_));
+  return MSF_OK;
+}
+
+msf_status Lane::launch_detect() {
   const char* det = static_cast<const char*>(table_.p) + sizeof(SlotPass) * B_;
   MSF_CUDA(launch_slot_detect(det, B_, max_chunks_, nx_, ny_, partial_.as<double>(), true,
                               stream_));
   return MSF_OK;
 }
 
-msf_status Lane::capture() {
+namespace {
+template <typename F>
+msf_status capture_graph(cudaStream_t stream, F&& enqueue, cudaGraphExec_t* out) {
   cudaGraph_t graph;
-  MSF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-  msf_status st = launch_step();
-  cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+  MSF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  msf_status st = enqueue();
+  cudaError_t ce = cudaStreamEndCapture(stream, &graph);
   if (st != MSF_OK) return st;
   MSF_CUDA(ce);
-  MSF_CUDA(cudaGraphInstantiate(&graph_, graph, 0));
+  MSF_CUDA(cudaGraphInstantiate(out, graph, 0));
   cudaGraphDestroy(graph);
   return MSF_OK;
+}
+}  // namespace
+
+msf_status Lane::capture_passes() {
+  return capture_graph(stream_, [this] { return launch_passes(); }, &graph_pass_);
+}
+
+msf_status Lane::capture_detect() {
+  return capture_graph(stream_, [this] { return launch_detect(); }, &graph_detect_);
 }
 
 msf_status Lane::step() {
@@ -207,18 +223,31 @@ msf_status Lane::step() {
     de[k] = e;
   }
   *dt = t;
-  MSF_CUDA(cudaMemcpyAsync(table_.p, h, table_bytes_, cudaMemcpyHostToDevice, stream_));
+  // the slot part always; the detection part when some slot finishes
+  const size_t pass_bytes = sizeof(SlotPass) * B_;
+  const size_t det_bytes = t.n_done ? sizeof(DetectTable) + sizeof(DetectSlot) * t.n_done : 0;
+  MSF_CUDA(cudaMemcpyAsync(table_.p, h, pass_bytes + det_bytes, cudaMemcpyHostToDevice,
+                           stream_));
   MSF_CUDA(cudaEventRecord(ring_ev_[r], stream_));
 
   // the first step runs its launches directly (kernel attributes are set
-  // on first use); later steps replay the captured graph
-  if (ctx_->graphs && steps_ >= 1 && !graph_) MSF_TRY(capture());
-  if (graph_) {
-    MSF_CUDA(cudaGraphLaunch(graph_, stream_));
+  // on first use); later steps replay the captured graphs
+  if (ctx_->graphs && steps_ >= 1 && !graph_pass_) MSF_TRY(capture_passes());
+  if (graph_pass_) {
+    MSF_CUDA(cudaGraphLaunch(graph_pass_, stream_));
   } else {
-    MSF_TRY(launch_step());
+    MSF_TRY(launch_passes());
   }
-  launches_ += 5;
+  launches_ += 2;
+  if (t.n_done) {
+    if (ctx_->graphs && steps_ >= 1 && !graph_detect_) MSF_TRY(capture_detect());
+    if (graph_detect_) {
+      MSF_CUDA(cudaGraphLaunch(graph_detect_, stream_));
+    } else {
+      MSF_TRY(launch_detect());
+    }
+    launches_ += 3;
+  }
   ++steps_;
 
   // advance every active slot by one slice

@@ -9,8 +9,9 @@
 //
 // Per step the host writes one table (SlotPass per slot, then the
 // detection entries) into a pinned ring and copies it to a fixed device
-// table; the three launches of a step read only that table, so they are
-// captured once as a CUDA graph and replayed.
+// table; the launches of a step read only that table, so they are captured
+// once as two CUDA graphs (the passes; the detection, replayed only on steps
+// where some slot finishes) and replayed.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -70,8 +71,10 @@ class Lane {
     int64_t probe = -1;
     int s = 0;
   };
-  msf_status capture();
-  msf_status launch_step();
+  msf_status capture_passes();
+  msf_status capture_detect();
+  msf_status launch_passes();
+  msf_status launch_detect();
   msf_status grow_chunks(int n_chunks);
 
   msf_context* ctx_;
@@ -87,7 +90,8 @@ class Lane {
   static constexpr int kRing = 4;
   unsigned char* host_ring_ = nullptr;  // kRing pinned tables
   cudaEvent_t ring_ev_[kRing] = {};
-  cudaGraphExec_t graph_ = nullptr;
+  cudaGraphExec_t graph_pass_ = nullptr;    // row + column pass
+  cudaGraphExec_t graph_detect_ = nullptr;  // detection of finished slots
   std::vector<Slot> slot_;
   std::deque<SlotJob*> queue_;
   int active_ = 0;

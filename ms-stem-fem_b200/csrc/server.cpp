@@ -93,7 +93,7 @@ using namespace msf;
 struct msf_server {
   msf_options opt{};
   msf_context* ctx = nullptr;
-  int slots = 64;
+  int slots = 0;  // per lane; 0: by grid size (lane_slots)
   int64_t budget = 0;
   std::thread worker;
   std::mutex mu;
@@ -149,7 +149,9 @@ struct msf_server {
     const std::pair<int, int> key{r.grid.nx, r.grid.ny};
     auto it = lanes.find(key);
     if (it == lanes.end()) {
-      auto lane = std::make_unique<Lane>(ctx, r.grid.nx, r.grid.ny, slots);
+      const int b = lane_slots(slots, (int64_t)r.grid.nx * r.grid.ny, (int)lanes.size() + 1,
+                               1 << 30);
+      auto lane = std::make_unique<Lane>(ctx, r.grid.nx, r.grid.ny, b);
       st = lane->init();
       if (st != MSF_OK) return st;
       it = lanes.emplace(key, std::move(lane)).first;
@@ -318,7 +320,7 @@ msf_status msf_server_create(const msf_options* opt, int32_t slots, msf_server**
     delete s;
     return st;
   }
-  s->slots = slots > 0 ? slots : 64;
+  s->slots = slots > 0 ? slots : 0;
   if (o.hbm_budget > 0) {
     s->budget = o.hbm_budget;
   } else {

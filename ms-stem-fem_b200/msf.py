@@ -42,7 +42,7 @@ EXPORTED = [
     "msf_time_passes", "msf_context_transfer_bytes", "msf_probe_noalloc",
     "msf_run_batch", "msf_server_create", "msf_server_submit", "msf_server_poll",
     "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
-    "msf_finish",
+    "msf_finish", "msf_run_plain", "msf_amorphous_positions",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -138,6 +138,10 @@ def lib() -> C.CDLL:
         L.msf_run.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics), C.POINTER(Raster),
                               C.POINTER(Detect), C.POINTER(Results)]
         L.msf_probe.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics), _dp]
+        L.msf_amorphous_positions.argtypes = [C.c_int64, _dp, C.c_double, C.c_uint64,
+                                              C.c_int64, _dp]
+        L.msf_run_plain.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics),
+                                    C.POINTER(Raster), C.POINTER(Detect), C.POINTER(Results)]
         L.msf_wavelength.argtypes = [C.c_double, _dp, _dp]
         L.msf_wavelength.restype = None
         L.msf_scherzer.argtypes = [C.c_int32, C.c_double, C.c_double]
@@ -312,6 +316,17 @@ class Context:
         out.finish(raster, detect)
         return out
 
+    def run_plain(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
+                  want_final_psi=False, cap_k=8192) -> "RunResult":
+        """The raster one probe at a time, one launch per reference step
+        (msf_run_plain; FP64 contexts)."""
+        out = RunResult(raster.n_x * raster.n_y, cap_k, spec.grid.nx, spec.grid.ny,
+                        want_final_psi, False)
+        _check(lib().msf_run_plain(self._h, spec._h, C.byref(optics), C.byref(raster),
+                                   C.byref(detect), C.byref(out._struct)))
+        out.finish(raster, detect)
+        return out
+
     def run_batch(self, jobs, slots=0, want_means=False, want_rings=False, cap_k=8192):
         """Several rasters through slot lanes (msf_run_batch).
 
@@ -365,6 +380,16 @@ class Context:
         out = np.zeros(2 * spec.grid.nx * spec.grid.ny)
         _check(lib().msf_probe(self._h, spec._h, C.byref(optics), _p(out)))
         return out.reshape(spec.grid.nx, spec.grid.ny, 2)
+
+
+def amorphous_positions(n_atoms: int, box, min_sep: float = 2.2, seed: int = 0,
+                        max_proposals: int = 0) -> np.ndarray:
+    """Seeded random-sequential-addition positions ((n_atoms, 3), host C++;
+    msf_amorphous_positions)."""
+    q = np.zeros((n_atoms, 3))
+    b = np.ascontiguousarray(box, dtype=np.float64)
+    _check(lib().msf_amorphous_positions(n_atoms, _p(b), min_sep, seed, max_proposals, _p(q)))
+    return q
 
 
 def segment_count(grid: Grid, detect: Detect) -> int:
