@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MSF_ABI_VERSION 1
+#define MSF_ABI_VERSION 2
 
 typedef enum {
   MSF_OK = 0,
@@ -106,6 +106,15 @@ typedef struct {
   uint32_t outputs;        /* MSF_OUT_* bits                                   */
   double det_inner, det_outer; /* ADF detector angles [rad]                    */
   double dr;               /* --dr azimuthal_binning_size_factor               */
+  /* Detector modulation transfer function (mtf_file + mtf_sampling_rate,
+   * adfstem.cpp:236-453, 2272-2385): applied to |psi(k)| before the FEM sums
+   * when n_mtf > 0 and mtf_resolution != 0.  mtf[n_mtf] and
+   * mtf_domain_sqr[n_mtf] as tem.cpp:276-285 leaves them (domain squared
+   * after scaling by 0.5 * mtf_resolution). */
+  int32_t n_mtf;
+  const double* mtf;
+  const double* mtf_domain_sqr;
+  double mtf_resolution;   /* [pixels per 1/A]                                */
 } msf_detect;
 
 /* Caller-owned result buffers; any pointer may be NULL when not wanted. */

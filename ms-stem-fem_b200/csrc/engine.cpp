@@ -553,8 +553,92 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
     MSF_CUDA(cudaMemsetAsync(P->acc_a.p, 0, P->acc_a.bytes, ctx->stream));
     MSF_CUDA(cudaMemsetAsync(P->acc_i.p, 0, P->acc_i.bytes, ctx->stream));
   }
+  // detector MTF (adfstem.cpp:298-414): table -> 2-D, BACKWARD transform,
+  // band limit applied to that real-space array (kept as the reference does
+  // it), FORWARD transform, / NxNy
+  if (det->n_mtf > 0 && det->mtf_resolution != 0 && det->mtf && det->mtf_domain_sqr) {
+    P->mtf = true;
+    const std::vector<double> h =
+        mtf_2d(g, det->mtf, det->mtf_domain_sqr, det->n_mtf, det->mtf_resolution);
+    MSF_TRY(upload(ctx, &P->mtf2d, h));
+    PassArgs a;
+    a.psi = P->mtf2d.p;
+    a.batch_stride = plane;
+    a.nb = 1;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.scale = 1.0;
+    MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
+    MSF_CUDA(launch_row(true, ROW_INV, a, ctx->stream));
+    MSF_TRY(ctx->twiddles(g.nx, true, &a.tw));
+    MSF_CUDA(launch_col(true, COL_INV, a, ctx->stream));
+    MSF_CUDA(launch_bw_limit(P->mtf2d.as<double>(), spec->mask_lo.as<int32_t>(),
+                             spec->mask_hi.as<int32_t>(), g.nx, g.ny, ctx->stream));
+    MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
+    MSF_CUDA(launch_row(true, ROW_FWD, a, ctx->stream));
+    MSF_TRY(ctx->twiddles(g.nx, true, &a.tw));
+    MSF_CUDA(launch_col(true, COL_FWD, a, ctx->stream));
+    MSF_CUDA(launch_scale(P->mtf2d.as<double>(), plane, 1.0 / g.nxny, nullptr, ctx->stream));
+    P->setup_launches += 6;
+  }
   // the host vectors above are staged by pageable copies: complete them
   MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MSF_OK;
+}
+
+// The detector MTF of nb exit waves (adfstem.cpp:2272-2385) into FP64 planes
+// `out`: |psi(k)| with the direct beam blocked, BACKWARD transform, times the
+// MTF / s (reference update order), FORWARD transform, / s, band limit.
+msf_status mtf_stage(msf_context* ctx, const RasterPlan& P, bool fp64, const void* psi, int nb,
+                     const SplitK& sk, double* out, cudaStream_t st) {
+  const msf_specimen* spec = P.spec;
+  const Grid& g = spec->g;
+  const int64_t plane = P.plane;
+  SplitK k = sk;
+  k.nx = g.nx;
+  k.ny = g.ny;
+  MSF_CUDA(launch_mtf_magnitude(fp64, psi, plane, nb, spec->kx.as<double>(), spec->ky.as<double>(),
+                                g.lambda * g.lambda, P.optics.alpha_max * P.optics.alpha_max, k,
+                                out, st));
+  PassArgs a;
+  a.psi = out;
+  a.batch_stride = plane;
+  a.nb = nb;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  a.scale = 1.0;
+  const void *tw_y = nullptr, *tw_x = nullptr;
+  MSF_TRY(ctx->twiddles(g.ny, true, &tw_y));
+  MSF_TRY(ctx->twiddles(g.nx, true, &tw_x));
+  a.tw = tw_y;
+  MSF_CUDA(launch_row(true, ROW_INV, a, st));
+  a.tw = tw_x;
+  MSF_CUDA(launch_col(true, COL_INV, a, st));
+  MSF_CUDA(launch_mtf_multiply(out, P.mtf2d.as<double>(), plane, nb, 1.0 / g.s, st));
+  a.tw = tw_y;
+  MSF_CUDA(launch_row(true, ROW_FWD, a, st));
+  a.tw = tw_x;
+  MSF_CUDA(launch_col(true, COL_FWD, a, st));
+  MSF_CUDA(launch_scale(out, plane * nb, 1.0 / g.s, nullptr, st));
+  MSF_CUDA(launch_bw_limit(out, spec->mask_lo.as<int32_t>(), spec->mask_hi.as<int32_t>(), g.nx,
+                           g.ny, st, nb));
+  return MSF_OK;
+}
+
+// Ring sums of the MTF-filtered waves replace the first n_k columns of the
+// batch's rows (the ADF column keeps the unfiltered sums, adfstem.cpp:2245).
+msf_status mtf_ring_sums(const RasterPlan& P, const SegmentPlan& seg, const double* mtf_psi,
+                         int nb, double* scratch_amp, double* scratch_int, double* amp_out,
+                         double* int_out, cudaStream_t st) {
+  if (P.n_k <= 0) return MSF_OK;
+  SplitK none;
+  MSF_CUDA(launch_segment_sums(true, mtf_psi, P.plane, nb, seg, scratch_amp, scratch_int, none,
+                               st));
+  const size_t pitch = sizeof(double) * P.n_seg, width = sizeof(double) * P.n_k;
+  MSF_CUDA(cudaMemcpy2DAsync(amp_out, pitch, scratch_amp, pitch, width, nb,
+                             cudaMemcpyDeviceToDevice, st));
+  MSF_CUDA(cudaMemcpy2DAsync(int_out, pitch, scratch_int, pitch, width, nb,
+                             cudaMemcpyDeviceToDevice, st));
   return MSF_OK;
 }
 
@@ -720,9 +804,14 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
     B = (int)std::max<int64_t>(1, std::min<int64_t>(cap, 64));
   }
   B = (int)std::min<int64_t>(B, n_probes);
-  DevBuf psi, d_partial;
+  DevBuf psi, d_partial, mtf_psi, mtf_amp, mtf_int;
   MSF_TRY(ctx->alloc(&psi, cbytes * plane * B));
   MSF_TRY(ctx->alloc(&d_partial, sizeof(double) * 2 * B * std::max(P.n_chunks, 1)));
+  if (P.mtf) {
+    MSF_TRY(ctx->alloc(&mtf_psi, 16 * plane * B));
+    MSF_TRY(ctx->alloc(&mtf_amp, sizeof(double) * B * n_seg));
+    MSF_TRY(ctx->alloc(&mtf_int, sizeof(double) * B * n_seg));
+  }
   SegmentPlan seg;
   seg.idx = P.seg_idx.as<int32_t>();
   seg.chunk_begin = P.chunk_begin.as<int32_t>();
@@ -791,9 +880,17 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
     }
     MSF_CUDA(launch_segment_sums(fp64, psi.p, plane, nb, seg, amp_out, int_out, sk,
                                  ctx->stream));
-    if (P.pix_modes)
+    if (P.mtf) {
+      MSF_TRY(mtf_stage(ctx, P, fp64, psi.p, nb, sk, mtf_psi.as<double>(), ctx->stream));
+      MSF_TRY(mtf_ring_sums(P, seg, mtf_psi.as<double>(), nb, mtf_amp.as<double>(),
+                            mtf_int.as<double>(), amp_out, int_out, ctx->stream));
+      if (P.pix_modes)
+        MSF_CUDA(launch_pixel_accum(true, mtf_psi.p, plane, nb, plane, P.acc_a.as<double>(),
+                                    P.acc_i.as<double>(), SplitK{}, ctx->stream));
+    } else if (P.pix_modes) {
       MSF_CUDA(launch_pixel_accum(fp64, psi.p, plane, nb, plane, P.acc_a.as<double>(),
                                   P.acc_i.as<double>(), sk, ctx->stream));
+    }
     return MSF_OK;
   };
 
@@ -881,8 +978,11 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
     // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:
     // 2*S slice passes, the segment sums (chunks, totals) and (pixel modes)
     // the accumulation
+    // (MTF: magnitude, 4 transform passes, multiply, scale, band limit and
+    // the ring sums of the filtered waves)
     res->kernel_launches =
-        P.setup_launches + n_batches * (2 * S + 2 + (P.pix_modes ? 1 : 0));
+        P.setup_launches +
+        n_batches * (2 * S + 2 + (P.pix_modes ? 1 : 0) + (P.mtf ? 8 + (P.n_k > 0 ? 2 : 0) : 0));
   }
   return MSF_OK;
 }
@@ -910,9 +1010,14 @@ msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
   const int64_t plane = P.plane;
   const int S = P.S;
   cudaStream_t st = ctx->stream;
-  DevBuf psi, d_partial;
+  DevBuf psi, d_partial, mtf_psi, mtf_amp, mtf_int;
   MSF_TRY(ctx->alloc(&psi, 16 * plane));
   MSF_TRY(ctx->alloc(&d_partial, sizeof(double) * 2 * std::max(P.n_chunks, 1)));
+  if (P.mtf) {
+    MSF_TRY(ctx->alloc(&mtf_psi, 16 * plane));
+    MSF_TRY(ctx->alloc(&mtf_amp, sizeof(double) * P.n_seg));
+    MSF_TRY(ctx->alloc(&mtf_int, sizeof(double) * P.n_seg));
+  }
   SegmentPlan seg;
   seg.idx = P.seg_idx.as<int32_t>();
   seg.chunk_begin = P.chunk_begin.as<int32_t>();
@@ -965,11 +1070,20 @@ msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
       launches += 8;
     }
     SplitK none;
-    MSF_CUDA(launch_segment_sums(true, d, plane, 1, seg, P.amp.as<double>() + p * P.n_seg,
-                                 P.inten.as<double>() + p * P.n_seg, none, st));
+    double* amp_p = P.amp.as<double>() + p * P.n_seg;
+    double* int_p = P.inten.as<double>() + p * P.n_seg;
+    MSF_CUDA(launch_segment_sums(true, d, plane, 1, seg, amp_p, int_p, none, st));
     launches += 2;
+    const double* fem_src = d;
+    if (P.mtf) {
+      MSF_TRY(mtf_stage(ctx, P, true, d, 1, none, mtf_psi.as<double>(), st));
+      MSF_TRY(mtf_ring_sums(P, seg, mtf_psi.as<double>(), 1, mtf_amp.as<double>(),
+                            mtf_int.as<double>(), amp_p, int_p, st));
+      fem_src = mtf_psi.as<double>();
+      launches += 8 + (P.n_k > 0 ? 2 : 0);
+    }
     if (P.pix_modes) {
-      MSF_CUDA(launch_pixel_accum(true, d, plane, 1, plane, P.acc_a.as<double>(),
+      MSF_CUDA(launch_pixel_accum(true, fem_src, plane, 1, plane, P.acc_a.as<double>(),
                                   P.acc_i.as<double>(), none, st));
       launches += 1;
     }

@@ -98,11 +98,13 @@ struct RasterPlan {
   DevBuf seg_idx, chunk_begin, seg_chunk;  // segments cut into chunks
   DevBuf amp, inten;            // [n_probes][n_seg] sums of |psi| and |psi|^2
   DevBuf acc_a, acc_i;          // [plane] sums over probes (pixel modes)
+  bool mtf = false;             // detector MTF applied before the FEM sums
+  DevBuf mtf2d;                 // [plane] complex FP64, band-limited as the reference does
   int64_t setup_launches = 0;
   int64_t device_bytes() const {
     return (int64_t)(d_shifts.bytes + probe64.bytes + psi0_tab.bytes + psi0k.bytes +
                      seg_idx.bytes + chunk_begin.bytes + seg_chunk.bytes + amp.bytes +
-                     inten.bytes + acc_a.bytes + acc_i.bytes);
+                     inten.bytes + acc_a.bytes + acc_i.bytes + mtf2d.bytes);
   }
 };
 // Device bytes plan_raster will allocate (for admission by an HBM budget).

@@ -58,6 +58,7 @@ struct msf_job {
   unsigned dupe_x = 1, dupe_y = 1, dupe_z = 1;
   std::string lammps_pre;
   unsigned lammps_steps = 0, lammps_samples = 0;
+  std::vector<double> mtf, mtf_domain;  // mtf_file: MTF values and domain
   // specimen
   std::vector<double> q;
   std::vector<uint32_t> z;
@@ -84,6 +85,37 @@ void parse_into(const std::string& s, T& v) {
 }
 
 bool blank(const std::string& l) { return l.find_first_not_of(" \t") == std::string::npos; }
+
+// read_mtf_file (tem_io.cpp:5722-5857): first line the domain, second line
+// the MTF, commas read as spaces; each line is read by extracting until the
+// stream reports eof (a trailing blank adds one more value, as there), and a
+// line counts only if the stream is still good after reading it.
+bool read_mtf(const std::string& name, msf_job* j) {
+  std::ifstream in(name.c_str());
+  if (!in.is_open()) {
+    j->messages += "Error opening MTF file: " + name + "\n";
+    return false;
+  }
+  auto values = [](std::string line, std::vector<double>* out) {
+    for (size_t at = line.find(','); at != std::string::npos; at = line.find(','))
+      line.replace(at, 1, " ");
+    std::istringstream ls(line);
+    double v;
+    while (!ls.eof()) {
+      ls >> v;
+      out->push_back(v);
+    }
+  };
+  std::string line;
+  if (std::getline(in, line) && in.good()) values(line, &j->mtf_domain);
+  if (std::getline(in, line) && in.good()) values(line, &j->mtf);
+  if (j->mtf_domain.size() != j->mtf.size()) {
+    j->messages += "Error reading MTF file: " + name + "\n MTF (1st line) and MTF domain (2nd "
+                   "line) do not have the same number of elements.\n";
+    return false;
+  }
+  return true;
+}
 
 // getline that skips whitespace-only lines, as the reference's readers do
 bool next_line(std::istream& in, std::string& line) {
@@ -127,8 +159,14 @@ bool parse_param_file(const std::string& path, msf_job* j) {
       if (j->det_inner > j->det_outer) std::swap(j->det_inner, j->det_outer);
       f.adfstem_detector_angles = 1;
     } else if (key == "mtf_file") {
-      j->messages += "Error, the MTF detector model (mtf_file) is not supported by this build\n";
-      f.fail = 1;
+      std::string name;
+      ls >> name;
+      if (!read_mtf(name, j)) {
+        j->messages += "Error, could not read MTF file : " + name + "\n";
+        f.fail = 1;
+      } else {
+        f.mtf_file = 1;
+      }
     } else if (key == "mtf_sampling_rate") {
       j->mtf_resolution = 0;
       if (!ls.eof()) ls >> j->mtf_resolution;
@@ -187,9 +225,15 @@ void parse_args(const std::vector<std::string>& args, msf_job* j) {
       f.pf = 1;
       idx += 1;
     } else if (a == "--mtf_file") {
-      // the reference reads the file but does not consume the argument
-      j->messages += "Error, the MTF detector model (--mtf_file) is not supported by this build\n";
-      f.fail = 1;
+      // the reference reads the file but does not consume the argument, so
+      // the file name is then rejected as an unexpected argument
+      const std::string name = has(1) ? args[idx + 1] : std::string();
+      if (!read_mtf(name, j)) {
+        j->messages += "Error, could not read MTF file : " + name + "\n";
+        f.fail = 1;
+      } else {
+        f.mtf_file = 1;
+      }
     } else if (a == "--mtf_sampling_rate") {
       j->mtf_resolution = 0;
       if (has(1)) { parse_into(args[idx + 1], j->mtf_resolution); idx += 1; }
@@ -429,6 +473,8 @@ namespace {
 // tem.cpp:405-1378 after the inputs are read
 msf_status finish_job(msf_job* j) {
   Flags& f = j->flags;
+  if (f.mtf_file && f.mtf_resolution)  // tem.cpp:276-285: domain in Nyquist units, squared
+    for (double& d : j->mtf_domain) d = std::pow((0.5 * j->mtf_resolution * d), 2);
   msf::wavelength(j->VV, &j->lambda, &j->gamma);
   const double xpd = j->xperiod * j->dupe_x, ypd = j->yperiod * j->dupe_y;
   double bw_pap = (j->nx / (2 * xpd) < j->ny / (2 * ypd)) ? j->nx / (2 * xpd) : j->ny / (2 * ypd);
@@ -665,6 +711,15 @@ msf_status msf_job_describe(const msf_job* j, msf_grid* grid, msf_atoms* atoms,
     det->det_inner = j->det_inner;
     det->det_outer = j->det_outer;
     det->dr = j->dr;
+    det->n_mtf = 0;
+    det->mtf = det->mtf_domain_sqr = nullptr;
+    det->mtf_resolution = 0;
+    if (f.mtf_file && f.mtf_resolution) {
+      det->n_mtf = (int32_t)j->mtf.size();
+      det->mtf = j->mtf.data();
+      det->mtf_domain_sqr = j->mtf_domain.data();
+      det->mtf_resolution = j->mtf_resolution;
+    }
   }
   return MSF_OK;
 }

@@ -565,6 +565,41 @@ __global__ void segment_reduce_kernel(const double* __restrict__ partial_a,
   }
 }
 
+// ---- detector MTF (adfstem.cpp:2272-2385) ------------------------------
+// out = |psi(k)| where lambda^2 k^2 > alpha_max^2 (the direct beam blocked),
+// else 0, as a real FP64 plane per probe.
+template <typename Real>
+__global__ void mtf_magnitude_kernel(const Cx<Real>* __restrict__ psi, int64_t stride, int nb,
+                                     const double* __restrict__ kx,
+                                     const double* __restrict__ ky, double lambda_sq,
+                                     double amax_sq, const SplitK sk, double2* out) {
+  const int64_t plane = (int64_t)sk.nx * sk.ny;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= plane * nb) return;
+  const int b = (int)(k / plane);
+  const int p = (int)(k - (int64_t)b * plane);
+  const int i = p / sk.ny, j = p - (p / sk.ny) * sk.ny;
+  double m = 0.0;
+  if (__dmul_rn(lambda_sq, ksq_exact(kx[i], ky[j])) > amax_sq) {
+    const int sx = sk.psi0k ? sk.shifts[2 * b] : 0, sy = sk.psi0k ? sk.shifts[2 * b + 1] : 0;
+    const double2 v = exit_value<Real>(psi + (int64_t)b * stride, p, sk, sx, sy);
+    m = sqrt(v.x * v.x + v.y * v.y);
+  }
+  out[k] = make_double2(m, 0.0);
+}
+
+// psi <- psi * mtf / s with the reference's in-place update order (the new
+// real part feeds the imaginary part), nb planes
+__global__ void mtf_multiply_kernel(double2* __restrict__ psi, const double2* __restrict__ mtf,
+                                    int64_t plane, int nb, double inv_s) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= plane * nb) return;
+  const double2 v = psi[k], m = mtf[k % plane];
+  const double re = (v.x * m.x - v.y * m.y) * inv_s;
+  const double im = (re * m.y + v.y * m.x) * inv_s;
+  psi[k] = make_double2(re, im);
+}
+
 // ---- slot batches: detection of the slots that finished -------------
 __device__ __forceinline__ const DetectSlot* detect_entries(const void* table) {
   return reinterpret_cast<const DetectSlot*>(static_cast<const char*>(table) +
@@ -713,10 +748,12 @@ __global__ void transmit_kernel(double2* __restrict__ psi, const double2* __rest
 // zero outside the band limit (bw_limit.cpp:30-47): column j keeps rows
 // i < lo[j] and i >= hi[j]
 __global__ void bw_limit_kernel(double2* __restrict__ psi, const int32_t* __restrict__ lo,
-                                const int32_t* __restrict__ hi, int nx, int ny) {
+                                const int32_t* __restrict__ hi, int nx, int ny, int nb) {
+  const int64_t plane = (int64_t)nx * ny;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (int64_t)nx * ny) return;
-  const int i = (int)(k / ny), j = (int)(k - (int64_t)i * ny);
+  if (k >= plane * nb) return;
+  const int64_t p = k % plane;
+  const int i = (int)(p / ny), j = (int)(p - (int64_t)i * ny);
   if (!(i < lo[j] || i >= hi[j])) psi[k] = make_double2(0.0, 0.0);
 }
 
@@ -879,9 +916,31 @@ cudaError_t launch_transmit(double* psi, const double* t, int64_t n, double inv_
 }
 
 cudaError_t launch_bw_limit(double* psi, const int32_t* lo, const int32_t* hi, int nx, int ny,
-                            cudaStream_t s) {
-  bw_limit_kernel<<<blocks_for((int64_t)nx * ny, 256), 256, 0, s>>>(
-      reinterpret_cast<double2*>(psi), lo, hi, nx, ny);
+                            cudaStream_t s, int nb) {
+  bw_limit_kernel<<<blocks_for((int64_t)nx * ny * nb, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(psi), lo, hi, nx, ny, nb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mtf_magnitude(bool fp64, const void* psi, int64_t stride, int nb,
+                                 const double* kx, const double* ky, double lambda_sq,
+                                 double amax_sq, const SplitK& sk, double* out, cudaStream_t s) {
+  const int64_t n = (int64_t)sk.nx * sk.ny * nb;
+  if (fp64)
+    mtf_magnitude_kernel<double><<<blocks_for(n, 256), 256, 0, s>>>(
+        static_cast<const double2*>(psi), stride, nb, kx, ky, lambda_sq, amax_sq, sk,
+        reinterpret_cast<double2*>(out));
+  else
+    mtf_magnitude_kernel<float><<<blocks_for(n, 256), 256, 0, s>>>(
+        static_cast<const float2*>(psi), stride, nb, kx, ky, lambda_sq, amax_sq, sk,
+        reinterpret_cast<double2*>(out));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mtf_multiply(double* psi, const double* mtf, int64_t plane, int nb,
+                                double inv_s, cudaStream_t s) {
+  mtf_multiply_kernel<<<blocks_for(plane * nb, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(psi), reinterpret_cast<const double2*>(mtf), plane, nb, inv_s);
   return cudaGetLastError();
 }
 

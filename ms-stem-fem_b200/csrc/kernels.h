@@ -189,9 +189,19 @@ cudaError_t launch_place_probe(double* psi, const double* probe, int nx, int ny,
 cudaError_t launch_transmit(double* psi, const double* t, int64_t n, double inv_s,
                             cudaStream_t s);
 cudaError_t launch_bw_limit(double* psi, const int32_t* lo, const int32_t* hi, int nx, int ny,
-                            cudaStream_t s);
+                            cudaStream_t s, int nb = 1);
 cudaError_t launch_propagate(double* psi, const double* px, const double* py, const int32_t* lo,
                              const int32_t* hi, int nx, int ny, cudaStream_t s);
+
+// ---- detector MTF (adfstem.cpp:2272-2385), FP64 planes ------------------
+// out[b] = |psi_b(k)| (exit wave incl. the vacuum part of split-wave runs)
+// where lambda^2 k^2 > alpha_max^2, else 0; imaginary parts 0.
+cudaError_t launch_mtf_magnitude(bool fp64, const void* psi, int64_t stride, int nb,
+                                 const double* kx, const double* ky, double lambda_sq,
+                                 double amax_sq, const SplitK& sk, double* out, cudaStream_t s);
+// psi_b <- psi_b * mtf / s (reference update order), nb planes.
+cudaError_t launch_mtf_multiply(double* psi, const double* mtf, int64_t plane, int nb,
+                                double inv_s, cudaStream_t s);
 
 // acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,

@@ -99,6 +99,10 @@ msf_status Lane::add(SlotJob* job) {
     set_error("raster grid does not match the lane");
     return MSF_ERR_ARG;
   }
+  if (job->plan.mtf) {
+    set_error("rasters with a detector MTF run through msf_run, not slot lanes");
+    return MSF_ERR_UNSUPPORTED;
+  }
   if (job->plan.n_chunks > max_chunks_) MSF_TRY(grow_chunks(job->plan.n_chunks));
   row_.inv_s = col_.inv_s = 1.0 / g.s;
   job->next_probe = 0;

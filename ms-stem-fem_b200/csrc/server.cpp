@@ -52,10 +52,10 @@ struct Stored {
 struct Request {
   uint64_t ticket = 0;
   msf_grid grid{};
-  std::vector<double> q, xp, yp;
+  std::vector<double> q, xp, yp, mtf, mtf_domain_sqr;
   std::vector<uint32_t> z;
   msf_optics optics{};
-  msf_detect det{};
+  msf_detect det{};  // its MTF pointers are set to the copies above at admission
   double t_submit = 0;
 };
 
@@ -144,6 +144,8 @@ struct msf_server {
     raster.n_y = (int32_t)r.yp.size();
     raster.x_p = r.xp.data();
     raster.y_p = r.yp.data();
+    r.det.mtf = r.mtf.empty() ? nullptr : r.mtf.data();
+    r.det.mtf_domain_sqr = r.mtf_domain_sqr.empty() ? nullptr : r.mtf_domain_sqr.data();
     st = plan_raster(ctx, out->spec.get(), &r.optics, &raster, &r.det, &out->job->plan);
     if (st != MSF_OK) return st;
     const std::pair<int, int> key{r.grid.nx, r.grid.ny};
@@ -349,6 +351,13 @@ msf_status msf_server_submit(msf_server* s, const msf_request* req, uint64_t* ti
   r.yp.assign(req->raster.y_p, req->raster.y_p + req->raster.n_y);
   r.optics = req->optics;
   r.det = req->detect;
+  if (r.det.n_mtf > 0 && r.det.mtf && r.det.mtf_domain_sqr) {
+    r.mtf.assign(r.det.mtf, r.det.mtf + r.det.n_mtf);
+    r.mtf_domain_sqr.assign(r.det.mtf_domain_sqr, r.det.mtf_domain_sqr + r.det.n_mtf);
+  } else {
+    r.det.n_mtf = 0;
+  }
+  r.det.mtf = r.det.mtf_domain_sqr = nullptr;
   r.t_submit = now_s();
   {
     std::lock_guard<std::mutex> lk(s->mu);

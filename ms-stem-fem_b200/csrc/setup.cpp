@@ -243,3 +243,33 @@ const double* kirkland_params(unsigned z) {
 }
 
 }  // namespace msf
+
+namespace msf {
+
+std::vector<double> mtf_2d(const Grid& g, const double* mtf, const double* domain_sqr, int n,
+                           double resolution) {
+  std::vector<double> out(2 * (size_t)g.nx * g.ny, 0.0);
+  const double nx = (double)g.nx, ny = (double)g.ny;
+  for (int i = 0; i < g.nx; ++i)
+    for (int j = 0; j < g.ny; ++j) {
+      const double xxx = std::pow(g.xpd, 2) * g.kx[i] / nx;
+      const double yyy = std::pow(g.ypd, 2) * g.ky[j] / ny;
+      const double rsqr = std::pow(xxx, 2) + std::pow(yyy, 2);
+      double v = 0.0;
+      for (int k = 0; k + 1 < n; ++k) {
+        if (rsqr >= domain_sqr[k] && rsqr < domain_sqr[k + 1]) {
+          const double d1 = std::sqrt(domain_sqr[k]), d2 = std::sqrt(domain_sqr[k + 1]);
+          v = mtf[k] + (mtf[k + 1] - mtf[k]) * (std::sqrt(rsqr) - d1) / (d2 - d1);
+          double arg = xxx / resolution;
+          const double sx = arg != 0 ? std::sin(arg) / arg : 1;
+          arg = yyy / resolution;
+          const double sy = arg != 0 ? std::sin(arg) / arg : 1;
+          v = v * sx * sy;
+        }
+      }
+      out[2 * ((size_t)i * g.ny + j)] = v;
+    }
+  return out;
+}
+
+}  // namespace msf

@@ -74,6 +74,14 @@ struct Rings {
 };
 Rings make_rings(const Grid& g, double dr);
 
+// Two-dimensional detector MTF before its band limiting (adfstem.cpp:298-384):
+// interleaved complex [nx][ny], real part interpolated from (mtf,
+// domain_sqr) at r^2 = (xpd^2 kx/Nx)^2 + (ypd^2 ky/Ny)^2 and multiplied by
+// sinc(xpd^2 kx/Nx / res) sinc(ypd^2 ky/Ny / res) where r^2 lies in the table;
+// 0 elsewhere.  Every table interval is tested (the last match wins).
+std::vector<double> mtf_2d(const Grid& g, const double* mtf, const double* domain_sqr, int n,
+                           double resolution);
+
 // ADF detector pixels k1 < kx*kx+ky*ky <= k2 (func.cpp:2593-2640).
 std::vector<int32_t> detector_pixels(const Grid& g, double k1, double k2);
 

@@ -79,7 +79,8 @@ class Raster(C.Structure):
 
 class Detect(C.Structure):
     _fields_ = [("outputs", C.c_uint32), ("det_inner", C.c_double),
-                ("det_outer", C.c_double), ("dr", C.c_double)]
+                ("det_outer", C.c_double), ("dr", C.c_double), ("n_mtf", C.c_int32),
+                ("mtf", _dp), ("mtf_domain_sqr", _dp), ("mtf_resolution", C.c_double)]
 
 
 class Results(C.Structure):

@@ -2,6 +2,7 @@
 everything else runs on the CPU (oracle, host logic, parsing, C-ABI load)."""
 import hashlib
 import json
+import re
 import shutil
 import sys
 from pathlib import Path
@@ -52,7 +53,20 @@ def case_dir(name, tmp_root: Path) -> Path:
             assert digest == meta["specimen_sha256"], "regenerated specimen differs"
             _SPEC_CACHE[name] = gen
         shutil.copy(_SPEC_CACHE[name], target)
+    files = meta.get("files", {})
+    for fname, text in files.items():  # parameter / MTF files, names made absolute
+        for other in files:
+            text = re.sub(r"(?<![\w./])%s(?![\w.])" % re.escape(other), str(d / other), text)
+        (d / fname).write_text(text)
     return d
+
+
+def case_argv(name, d):
+    """The case's argv with its specimen and extra files named by absolute
+    path inside the case directory `d`."""
+    meta, _ = load_case(name)
+    local = {meta["argv"][1]} | set(meta.get("files", {}))
+    return [str(d / a) if a in local else a for a in meta["argv"]]
 
 
 @pytest.fixture(scope="session")

@@ -70,6 +70,18 @@ CASES = {
                  "-m 1024 1024 200000 --adfstemuncorrfem --V_omega --V_re --cs3 1.3e7 "
                  "--defocus 0 --alphamax 0.0015 --rasterspacing 50 --minslice 2.0 --dr 1.2065",
                  False, None),
+    # detector MTF: only the parameter-file route works in the reference (its
+    # --mtf_file option does not consume its argument); FEM pixel modes too
+    "mtf": (dict(n=780, box=(25, 25, 25), seed=1),
+            "--parameter_file mtf.param -m 128 128 200000 --adfstemuncorrfem --V_omega --V_re "
+            "--Omega_vimage --cs3 1.3e7 --scherzer_defocus --alphamax 0.010 "
+            "--rasterspacing 6.25 --minslice 2.0 --images", True, None),
+}
+
+# extra input files of a case, written beside the specimen (name -> text)
+FILES = {
+    "mtf": {"mtf.param": "mtf_file mtf.csv\nmtf_sampling_rate 20\n",
+            "mtf.csv": "0, 0.25, 0.5, 0.75, 1.0, 1.5\n1.0, 0.8, 0.55, 0.35, 0.2, 0.1\n"},
 }
 
 
@@ -106,6 +118,8 @@ def run_case(name):
     work = Path(tempfile.mkdtemp(prefix="golden_" + name))
     spec = work / (name + ".data")
     make_specimen_file(recipe, spec)
+    for fname, text in FILES.get(name, {}).items():
+        (work / fname).write_text(text)
     argv = ["-a", spec.name, "--output_prefix", name] + args.split()
     env = {"MSF_REF_DUMP_SLICES": str(work / "slices.txt")}
     if tslice is not None:
@@ -131,7 +145,7 @@ def run_case(name):
         out["transmission"] = t
     np.savez_compressed(HERE / (name + ".npz"), **out)
     meta = dict(case=name, argv=argv, recipe=recipe, specimen_sha256=sha256(spec),
-                committed_specimen=commit, prefix=prefix.name,
+                committed_specimen=commit, prefix=prefix.name, files=FILES.get(name, {}),
                 adfstem_seconds=r["adfstem_seconds"], probes=r["probes"], slices=r["slices"])
     (HERE / (name + ".json")).write_text(json.dumps(meta, indent=1) + "\n")
     if commit:

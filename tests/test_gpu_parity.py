@@ -10,8 +10,8 @@ import pytest
 
 import msf
 import oracle
-from conftest import (ROOT, assert_variance_close, case_dir, golden_cases, load_case,
-                      rel_err)
+from conftest import (ROOT, assert_variance_close, case_argv, case_dir, golden_cases,
+                      load_case, rel_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +25,7 @@ MODES = ["V_omega", "Vbar_r", "V_re", "Omega_vimage", "V_gt17", "V_rbar"]
 def run_case(name, golden_tmp, precision, batch=0, graphs=True, want_psi=False):
     meta, ref = load_case(name)
     d = case_dir(name, golden_tmp)
-    argv = [a if a != meta["argv"][1] else str(d / a) for a in meta["argv"]]
+    argv = case_argv(name, d)
     job, spec, res, ctx = msf.run_job(argv, precision=precision, batch=batch, graphs=graphs,
                                       want_final_psi=want_psi)
     return meta, ref, job, spec, res, ctx

@@ -30,3 +30,19 @@ def test_plain_rejects_fp32_context():
     spec = ctx.specimen(j.grid, j.pos, j.z)
     with pytest.raises(msf.MsfError):
         ctx.run_plain(spec, j.optics, j.raster, j.detect)
+
+
+def test_plain_matches_reference_with_mtf(golden_tmp):
+    """The plain path with the detector MTF against the reference's own run
+    (golden case 'mtf', made through a parameter file)."""
+    from conftest import assert_variance_close, case_argv, case_dir, load_case, rel_err
+    meta, ref = load_case("mtf")
+    job = msf.Job(case_argv("mtf", case_dir("mtf", golden_tmp)))
+    assert job.detect.n_mtf > 0
+    ctx = msf.Context(precision="fp64")
+    q, z = job.positions()
+    spec = ctx.specimen(job.grid, q, z)
+    r = ctx.run_plain(spec, job.optics, job.raster, job.detect)
+    assert rel_err(r.adf_image, ref["adf_image"]).max() <= 1e-5
+    for mode in ("V_omega", "V_re", "Omega_vimage"):
+        assert_variance_close(r.v[mode], ref[mode][:, 1], 1e-5, 1e-12, what=mode)

@@ -9,7 +9,7 @@ import pytest
 
 import msf
 import oracle
-from conftest import ROOT, case_dir, golden_cases, load_case
+from conftest import ROOT, case_argv, case_dir, golden_cases, load_case
 
 
 def declared_functions():
@@ -25,14 +25,14 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) == set(msf.EXPORTED)
-    assert lib.msf_abi_version() == 1
+    assert lib.msf_abi_version() == 2
 
 
 @pytest.mark.parametrize("name", golden_cases())
 def test_parse_matches_oracle_derivation(name, golden_tmp):
     meta, ref = load_case(name)
     d = case_dir(name, golden_tmp)
-    argv = [a if a != meta["argv"][1] else str(d / a) for a in meta["argv"]]
+    argv = case_argv(name, d)
     job = msf.Job(argv)
     ojob, q_or, z_or = oracle.job_from_argv(meta["argv"], d)
     assert job.grid.nx == ojob["nx"] and job.grid.ny == ojob["ny"]
@@ -62,7 +62,7 @@ def test_slicing_bit_exact(name, golden_tmp):
 def test_probe_shifts_and_ring_bins_bit_exact(name, golden_tmp):
     meta, _ = load_case(name)
     d = case_dir(name, golden_tmp)
-    argv = [a if a != meta["argv"][1] else str(d / a) for a in meta["argv"]]
+    argv = case_argv(name, d)
     job = msf.Job(argv)
     oj = job.oracle_job()
     sh = np.zeros(2 * job.n_probes, dtype=np.int64)
@@ -163,6 +163,48 @@ def test_parameter_file(golden_tmp):
                       "200000", "--parameter_file", str(pf2), "--adfstemuncorr",
                       "--scherzer_defocus", "--alphamax", "0.01"])
     assert "lacking required parameters" in err
+
+
+def test_mtf_file(golden_tmp, tmp_path):
+    """mtf_file / mtf_sampling_rate (tem_io.cpp:4214-4262, 5371-5440, 5722-5857;
+    tem.cpp:276-285): domain on line 1, MTF on line 2, domain rescaled to
+    (0.5 res d)^2; the CLI option reads the file without consuming its name."""
+    d = case_dir("fem128", golden_tmp)
+    spec = str(d / "fem128.data")
+    (tmp_path / "m.csv").write_text("0, 0.5, 1.0\n1.0, 0.6, 0.2\n")
+    (tmp_path / "m.param").write_text("mtf_file %s\nmtf_sampling_rate 20\n" % (tmp_path / "m.csv"))
+    base = ["-a", spec, "--output_prefix", str(d / "x"), "--parameter_file",
+            str(tmp_path / "m.param"), "-m", "128", "128", "200000", "--cs3", "1.3e7",
+            "--scherzer_defocus", "--alphamax", "0.01", "--adfstemuncorrfem"]
+    j = msf.Job(base)
+    det = j.detect
+    assert det.n_mtf == 3 and det.mtf_resolution == 20
+    assert [det.mtf[k] for k in range(3)] == [1.0, 0.6, 0.2]
+    assert [det.mtf_domain_sqr[k] for k in range(3)] == [(0.5 * 20 * v) ** 2
+                                                        for v in (0.0, 0.5, 1.0)]
+    # without a sampling rate the MTF is off and the run is refused (flags differ)
+    (tmp_path / "m2.param").write_text("mtf_file %s\n" % (tmp_path / "m.csv"))
+    base2 = list(base)
+    base2[base2.index(str(tmp_path / "m.param"))] = str(tmp_path / "m2.param")
+    assert "lacking required parameters" in _run_parse(base2)
+    # CLI: the file name is left behind as an unexpected argument
+    err = _run_parse(["-a", spec, "--output_prefix", "x", "-m", "128", "128", "200000",
+                      "--cs3", "1.3e7", "--scherzer_defocus", "--alphamax", "0.01",
+                      "--adfstemuncorrfem", "--mtf_file", str(tmp_path / "m.csv"),
+                      "--mtf_sampling_rate", "20"])
+    assert "unexpected argument : " + str(tmp_path / "m.csv") in err
+    # unequal lines, a missing second newline, a missing file
+    for text in ("0, 0.5\n1.0\n", "0, 0.5\n1.0, 0.5"):
+        (tmp_path / "bad.csv").write_text(text)
+        (tmp_path / "bad.param").write_text("mtf_file %s\nmtf_sampling_rate 20\n"
+                                            % (tmp_path / "bad.csv"))
+        b = list(base)
+        b[b.index(str(tmp_path / "m.param"))] = str(tmp_path / "bad.param")
+        assert "could not read MTF file" in _run_parse(b)
+    (tmp_path / "none.param").write_text("mtf_file %s\n" % (tmp_path / "none.csv"))
+    b = list(base)
+    b[b.index(str(tmp_path / "m.param"))] = str(tmp_path / "none.param")
+    assert "Error opening MTF file" in _run_parse(b)
 
 
 def test_lammps_reader_errors(tmp_path):
