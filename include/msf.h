@@ -58,7 +58,9 @@ typedef enum { MSF_FP64 = 0, MSF_FP32 = 1 } msf_precision;
 #define MSF_OUT_OMEGA_VIMAGE (1u << 4) /* --Omega_vimage (flags.d4)         */
 #define MSF_OUT_V_GT17       (1u << 5) /* --V_gt17      (flags.gt17)        */
 #define MSF_OUT_V_RBAR       (1u << 6) /* --V_rbar      (flags.rva)         */
-#define MSF_OUT_FEM_MASK     (0x7eu)
+#define MSF_OUT_CORRELOGRAPH (1u << 7) /* --correlograph (raster average)  */
+#define MSF_OUT_CORRELOGRAPH_VAR (1u << 8) /* --correlograph_variance      */
+#define MSF_OUT_FEM_MASK     (0x1feu)  /* every output that needs ring bins */
 
 typedef struct msf_context msf_context;
 typedef struct msf_specimen msf_specimen;
@@ -141,6 +143,17 @@ typedef struct {
                               kernels inside replayed graphs)                 */
   double seconds_setup;    /* out: specimen set-up time (msf_run: 0)           */
   double seconds_raster;   /* out: device time of the raster                   */
+  /* FEM correlograph (adfstem.cpp:2603-2685, 3617-3760): per probe and ring
+   * bin ii, per azimuthal bin jj, n_k * S(ii,jj) / S(ii) - 1 when that
+   * ratio is >= 1 (else 0), S(ii,jj) the sum of |psi(k)| over the cell and
+   * S(ii) over the ring; arrays [jj*n_k + ii], n_k*n_phi entries. */
+  int32_t cap_phi;         /* capacity: phi_lower holds cap_phi + 1 values,
+                              the arrays below cap_k * cap_phi (per probe)  */
+  int32_t n_phi;           /* out: number of azimuthal bins                    */
+  double* phi_lower;       /* out: n_phi + 1 azimuthal boundaries [rad]        */
+  double* correlograph;    /* out: raster average                              */
+  double* correlograph_sqr;/* out: sum over probes of the squares (variance)   */
+  double* correlograph_probes; /* out: n_x*n_y blocks of n_k*n_phi, raster order */
 } msf_results;
 
 /* ---- library ---------------------------------------------------------- */

@@ -207,7 +207,10 @@ int32_t msf_segment_count(const msf_grid* grid, const msf_detect* detect) {
   if (!grid || !detect) return -1;
   if (!(detect->outputs & MSF_OUT_FEM_MASK)) return 1;
   Grid g = grid_of(grid);
-  return make_rings(g, detect->dr).n_k + 1;
+  const Rings r = make_rings(g, detect->dr);
+  int32_t n = r.n_k + 1;
+  if (detect->outputs & MSF_OUT_CORRELOGRAPH) n += r.n_k * make_cells(g, r).n_phi;
+  return n;
 }
 
 msf_status msf_run_partial(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,

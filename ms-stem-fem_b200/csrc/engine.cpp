@@ -532,6 +532,15 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
   seg_idx.insert(seg_idx.end(), adf_pix.begin(), adf_pix.end());
   seg_start.push_back((int32_t)seg_idx.size());
   P->n_seg = P->n_k + 1;
+  if (P->fem && (det->outputs & MSF_OUT_CORRELOGRAPH)) {
+    // correlograph cells (k bin, phi bin) after the ADF annulus
+    const Cells cells = make_cells(g, P->rings);
+    const size_t n_cells = (size_t)P->n_k * cells.n_phi;
+    const int32_t base = (int32_t)seg_idx.size();
+    seg_idx.insert(seg_idx.end(), cells.pix.begin(), cells.pix.end());
+    for (size_t c = 0; c < n_cells; ++c) seg_start.push_back(base + cells.start[c + 1]);
+    P->n_seg += (int)n_cells;
+  }
   // chunks of at most kSegmentChunk pixels, never straddling two segments
   std::vector<int32_t> chunk_begin, seg_chunk;
   for (int gi = 0; gi < P->n_seg; ++gi) {
@@ -625,8 +634,9 @@ msf_status mtf_stage(msf_context* ctx, const RasterPlan& P, bool fp64, const voi
   return MSF_OK;
 }
 
-// Ring sums of the MTF-filtered waves replace the first n_k columns of the
-// batch's rows (the ADF column keeps the unfiltered sums, adfstem.cpp:2245).
+// Ring (and correlograph cell) sums of the MTF-filtered waves replace those
+// columns of the batch's rows; the ADF column (index n_k) keeps the
+// unfiltered sums (adfstem.cpp:2245).
 msf_status mtf_ring_sums(const RasterPlan& P, const SegmentPlan& seg, const double* mtf_psi,
                          int nb, double* scratch_amp, double* scratch_int, double* amp_out,
                          double* int_out, cudaStream_t st) {
@@ -634,11 +644,16 @@ msf_status mtf_ring_sums(const RasterPlan& P, const SegmentPlan& seg, const doub
   SplitK none;
   MSF_CUDA(launch_segment_sums(true, mtf_psi, P.plane, nb, seg, scratch_amp, scratch_int, none,
                                st));
-  const size_t pitch = sizeof(double) * P.n_seg, width = sizeof(double) * P.n_k;
-  MSF_CUDA(cudaMemcpy2DAsync(amp_out, pitch, scratch_amp, pitch, width, nb,
-                             cudaMemcpyDeviceToDevice, st));
-  MSF_CUDA(cudaMemcpy2DAsync(int_out, pitch, scratch_int, pitch, width, nb,
-                             cudaMemcpyDeviceToDevice, st));
+  const size_t pitch = sizeof(double) * P.n_seg;
+  const size_t spans[2][2] = {{0, (size_t)P.n_k}, {(size_t)P.n_k + 1, (size_t)P.n_seg}};
+  for (const auto& sp : spans) {
+    if (sp[1] <= sp[0]) continue;
+    const size_t off = sp[0], width = sizeof(double) * (sp[1] - sp[0]);
+    MSF_CUDA(cudaMemcpy2DAsync(amp_out + off, pitch, scratch_amp + off, pitch, width, nb,
+                               cudaMemcpyDeviceToDevice, st));
+    MSF_CUDA(cudaMemcpy2DAsync(int_out + off, pitch, scratch_int + off, pitch, width, nb,
+                               cudaMemcpyDeviceToDevice, st));
+  }
   return MSF_OK;
 }
 
@@ -687,7 +702,12 @@ msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& opti
   const uint32_t fem = detect.outputs & MSF_OUT_FEM_MASK;
   const bool pix_modes = detect.outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE |
                                            MSF_OUT_V_GT17 | MSF_OUT_V_RBAR);
-  const int n_k = fem ? rings.n_k : 0, n_seg = n_k + 1;
+  const bool corr = fem && (detect.outputs & MSF_OUT_CORRELOGRAPH);
+  const int n_k = fem ? rings.n_k : 0;
+  Cells cells;
+  if (corr) cells = make_cells(g, rings);
+  const int n_phi = corr ? cells.n_phi : 0;
+  const int n_seg = n_k + 1 + n_k * n_phi;
   if (pix_modes && fem && (!acc_a || !acc_i)) {
     set_error("pixel FEM modes need the per-pixel sums");
     return MSF_ERR_ARG;
@@ -717,6 +737,39 @@ msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& opti
       if (res->ring_intensity) res->ring_intensity[p * res->cap_k + k] = inten[p * n_seg + k];
     }
   const double n_r = (double)(size_t)n_probes;
+  if (corr) {  // adfstem.cpp:2603-2652, 3617-3633
+    if (n_phi > res->cap_phi) {
+      set_error("results.cap_phi is smaller than the number of azimuthal bins (" +
+                std::to_string(n_phi) + ")");
+      return MSF_ERR_ARG;
+    }
+    res->n_phi = n_phi;
+    if (res->phi_lower)
+      for (int jj = 0; jj <= n_phi && jj < (int)cells.phi_bounds.size(); ++jj)
+        res->phi_lower[jj] = cells.phi_bounds[jj];
+    const size_t nc = (size_t)n_k * n_phi;
+    std::vector<double> sum(nc, 0.0), sqr(nc, 0.0), one(nc);
+    for (int64_t p = 0; p < n_probes; ++p) {
+      const double* row = &amp[p * n_seg];
+      for (int ii = 0; ii < n_k; ++ii) {
+        const double S = inside[ii] ? 0.0 : row[ii];  // direct beam zeroed
+        for (int jj = 0; jj < n_phi; ++jj) {
+          const double Cv = inside[ii] ? 0.0 : row[n_k + 1 + (size_t)ii * n_phi + jj];
+          const size_t c = ii + (size_t)jj * n_k;
+          const double t = (cnt[ii] * Cv / S);
+          one[c] = (t >= 1 && cnt[ii] != 0 && Cv != 0 && S != 0) ? (cnt[ii] * Cv / S) - 1 : 0.0;
+          sum[c] += one[c];
+          sqr[c] += one[c] * one[c];
+        }
+      }
+      if (res->correlograph_probes)
+        std::memcpy(res->correlograph_probes + p * nc, one.data(), nc * sizeof(double));
+    }
+    for (size_t c = 0; c < nc; ++c) sum[c] = sum[c] / n_r;
+    if (res->correlograph) std::memcpy(res->correlograph, sum.data(), nc * sizeof(double));
+    if (res->correlograph_sqr && (detect.outputs & MSF_OUT_CORRELOGRAPH_VAR))
+      std::memcpy(res->correlograph_sqr, sqr.data(), nc * sizeof(double));
+  }
   if (det->outputs & (MSF_OUT_V_OMEGA | MSF_OUT_VBAR_R)) {
     std::vector<double> sa2(n_k, 0.0), sa(n_k, 0.0), vs(n_k, 0.0);
     for (int64_t p = 0; p < n_probes; ++p) {

@@ -354,10 +354,6 @@ void check_flags(msf_job* j) {
     j->messages += "Error: choose either aberration corrected or uncorrected modes\n";
     f.fail = 1;
   }
-  if (f.correlograph) {
-    j->messages += "Error, the correlograph outputs are not supported by this build\n";
-    f.fail = 1;
-  }
   if (f.lammps_preTEM_file) {
     j->messages += "Error, the LAMMPS-coupled FEM mode needs ms-stem-fem-md and LAMMPS, "
                    "which are not available in this build\n";
@@ -584,6 +580,26 @@ bool write_tif16(const std::string& name, const double* data, size_t height, siz
   return ok;
 }
 
+// output_correlograph_to_txt (io_txt.cpp:96-170): "0 " and the phi lower
+// boundaries on the first line, then per k bin its lower boundary and the
+// values [ii + jj*n_k], each followed by a space.
+bool write_correlograph_txt(const std::string& prefix, const double* data,
+                            const double* phi_lower, int n_phi, const double* k_lower,
+                            int n_k) {
+  FILE* fp = std::fopen((prefix + ".txt").c_str(), "w");
+  if (!fp) return false;
+  std::fprintf(fp, "0 ");
+  for (int jj = 0; jj < n_phi; ++jj) std::fprintf(fp, "%.10e ", phi_lower[jj]);
+  std::fprintf(fp, "\n");
+  for (int ii = 0; ii < n_k; ++ii) {
+    std::fprintf(fp, "%.10e ", k_lower[ii]);
+    for (int jj = 0; jj < n_phi; ++jj) std::fprintf(fp, "%.10e ", data[ii + (size_t)jj * n_k]);
+    std::fprintf(fp, "\n");
+  }
+  std::fclose(fp);
+  return true;
+}
+
 bool write_variance(const std::string& prefix, const double* k_lower, const double* v, int n) {
   FILE* fp = std::fopen((prefix + ".txt").c_str(), "w");
   if (!fp) return false;
@@ -707,6 +723,8 @@ msf_status msf_job_describe(const msf_job* j, msf_grid* grid, msf_atoms* atoms,
       if (f.d4) det->outputs |= MSF_OUT_OMEGA_VIMAGE;
       if (f.gt17) det->outputs |= MSF_OUT_V_GT17;
       if (f.rva) det->outputs |= MSF_OUT_V_RBAR;
+      if (f.correlograph) det->outputs |= MSF_OUT_CORRELOGRAPH;
+      if (f.correlograph_variance) det->outputs |= MSF_OUT_CORRELOGRAPH_VAR;
     }
     det->det_inner = j->det_inner;
     det->det_outer = j->det_outer;
@@ -740,6 +758,61 @@ msf_status msf_write_outputs(const msf_job* j, const msf_results* r) {
         msf::set_error("Unable to write variance to file: " + pre + m.name + ".txt");
         return MSF_ERR_IO;
       }
+  }
+  if (f.fem && f.correlograph && r->correlograph && r->phi_lower && r->k_lower) {
+    // adfstem.cpp:2652-2685, 3617-3760
+    const int n_k = r->n_k, n_phi = r->n_phi;
+    const size_t nc = (size_t)n_k * n_phi;
+    const double k_res = (n_k / (1.0 - 0.2)) * 1.0e8;
+    const double phi_res = (double)((unsigned)n_phi / 360);  // integer division, as there
+    auto image = [&](const std::string& name, const double* d, size_t h, size_t w, bool logscale) {
+      if (h * w == 0) return true;
+      double mn = d[0], mx = d[0];
+      for (size_t k = 0; k < h * w; ++k) { mx = std::max(mx, d[k]); mn = std::min(mn, d[k]); }
+      return write_tif16(name + (logscale ? "_logscale.tif" : ".tif"), d, h, w, mn, mx, logscale,
+                         phi_res, k_res, 3);
+    };
+    bool ok = true;
+    if (r->correlograph_probes && (f.correlograph_everyimage || f.correlograph_everytxt)) {
+      const size_t ny = j->y_p.size();
+      for (size_t p = 0; p < j->x_p.size() * ny && ok; ++p) {
+        const std::string name = pre + "_" + std::to_string(p / ny) + "_" + std::to_string(p % ny);
+        const double* c = r->correlograph_probes + p * nc;
+        if (f.correlograph_everyimage) ok = ok && image(name, c, n_phi, n_k, false);
+        if (f.correlograph_everytxt)
+          ok = ok && write_correlograph_txt(name, c, r->phi_lower, n_phi, r->k_lower, n_k);
+      }
+    }
+    ok = ok && write_correlograph_txt(pre + "_correlograph_avg", r->correlograph, r->phi_lower,
+                                      n_phi, r->k_lower, n_k) &&
+         image(pre + "_correlograph_avg", r->correlograph, n_phi, n_k, false);
+    if (ok && f.correlograph_variance && r->correlograph_sqr) {
+      // k bins of [0.2, 1.0]; boundary ii is ii * delta_k (adfstem.cpp:1020-1026)
+      auto bound = [&](int ii) { return ii < n_k ? r->k_lower[ii] : ii * r->k_lower[1]; };
+      size_t start = 0, end = n_k > 0 ? n_k - 1 : 0;
+      for (int ii = 0; ii < n_k; ++ii) {
+        if (bound(ii) <= 0.2 && bound(ii + 1) > 0.2) start = ii;
+        if (bound(ii) <= 1.0 && bound(ii + 1) > 1.0) end = ii;
+      }
+      const size_t n_red = end >= start ? end - start : 0;
+      const double n_r = (double)(j->x_p.size() * j->y_p.size());
+      std::vector<double> var(n_red * n_phi, 0.0);
+      for (size_t ii = start; ii < end; ++ii)
+        for (int jj = 0; jj < n_phi; ++jj) {
+          const size_t c = ii + (size_t)jj * n_k, d = (ii - start) + (size_t)jj * n_red;
+          const double sq = r->correlograph_sqr[c], av = r->correlograph[c];
+          const double t = sq / (n_r * av * av);
+          var[d] = (sq != 0 && n_r != 0 && av != 0 && t >= 1) ? t - 1 : 0;
+        }
+      ok = write_correlograph_txt(pre + "_correlograph_variance", r->correlograph_sqr,
+                                  r->phi_lower, n_phi, r->k_lower, n_k) &&
+           image(pre + "_correlograph_variance", var.data(), n_phi, n_red, true) &&
+           image(pre + "_correlograph_variance", var.data(), n_phi, n_red, false);
+    }
+    if (!ok) {
+      msf::set_error("could not write the correlograph outputs of " + pre);
+      return MSF_ERR_IO;
+    }
   }
   if (f.image_output && r->adf_image) {
     const size_t nx = j->x_p.size(), ny = j->y_p.size();
@@ -794,6 +867,28 @@ int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) 
     r.omega_vimage = v[3].data();
     r.v_gt17 = v[4].data();
     r.v_rbar = v[5].data();
+    // correlograph: bins from the segment counts with and without the cells
+    std::vector<double> phi, corr, corr_sqr, corr_probes;
+    if (det.outputs & MSF_OUT_CORRELOGRAPH) {
+      msf_detect plain = det;
+      plain.outputs &= ~(uint32_t)(MSF_OUT_CORRELOGRAPH | MSF_OUT_CORRELOGRAPH_VAR);
+      plain.outputs |= MSF_OUT_V_OMEGA;
+      const int32_t n_k = msf_segment_count(&grid, &plain) - 1;
+      const int32_t cells = msf_segment_count(&grid, &det) - 1 - n_k;
+      const int32_t n_phi = n_k > 0 ? cells / n_k : 0;
+      const size_t nc = std::max<size_t>(1, (size_t)n_k * n_phi);
+      phi.assign(n_phi + 1, 0.0);
+      corr.assign(nc, 0.0);
+      corr_sqr.assign(nc, 0.0);
+      r.cap_phi = n_phi;
+      r.phi_lower = phi.data();
+      r.correlograph = corr.data();
+      r.correlograph_sqr = corr_sqr.data();
+      if (j->flags.correlograph_everyimage || j->flags.correlograph_everytxt) {
+        corr_probes.assign(nc * nr, 0.0);
+        r.correlograph_probes = corr_probes.data();
+      }
+    }
     if ((st = msf_run(ctx, spec, &optics, &raster, &det, &r)) == MSF_OK &&
         (st = msf_write_outputs(j, &r)) == MSF_OK)
       rc = 0;

@@ -199,6 +199,46 @@ Rings make_rings(const Grid& g, double dr) {
   return r;
 }
 
+Cells make_cells(const Grid& g, const Rings& r) {
+  Cells c;
+  unsigned count = 0;
+  for (double b : r.bounds)
+    if (b >= 0.2 && b <= 1.0) ++count;
+  c.n_phi = count > 0 ? (int32_t)(count - 1) : 0;
+  const size_t n_cells = (size_t)r.n_k * c.n_phi;
+  c.start.assign(n_cells + 1, 0);
+  if (c.n_phi == 0) {
+    c.phi_bounds.assign(1, 0.0);
+    return c;
+  }
+  const double delta_phi = 2 * kPi / c.n_phi;
+  for (int32_t ii = 0; ii < c.n_phi + 1; ++ii) c.phi_bounds.push_back(ii * delta_phi);
+  // cell of every ring pixel, in ring order
+  std::vector<int32_t> cell_of(r.pix.size(), -1);
+  std::vector<int32_t> counts(n_cells, 0);
+  for (int32_t ii = 0; ii < r.n_k; ++ii)
+    for (int32_t q = r.start[ii]; q < r.start[ii + 1]; ++q) {
+      const int32_t p = r.pix[q];
+      const int i = p / g.ny, j = p % g.ny;
+      const double phi = kPi + std::atan2(g.ky[j], g.kx[i]);
+      double lower = c.phi_bounds[0];
+      for (int32_t jj = 0; jj < c.n_phi; ++jj) {
+        if (phi > lower && phi <= c.phi_bounds[jj + 1]) {
+          cell_of[q] = ii * c.n_phi + jj;
+          ++counts[(size_t)ii * c.n_phi + jj];
+          break;
+        }
+        lower = c.phi_bounds[jj];  // lags one boundary behind, as there
+      }
+    }
+  for (size_t k = 0; k < n_cells; ++k) c.start[k + 1] = c.start[k] + counts[k];
+  c.pix.assign(c.start[n_cells], 0);
+  std::vector<int32_t> fill(c.start.begin(), c.start.end() - 1);
+  for (size_t q = 0; q < r.pix.size(); ++q)
+    if (cell_of[q] >= 0) c.pix[fill[cell_of[q]]++] = r.pix[q];
+  return c;
+}
+
 std::vector<int32_t> detector_pixels(const Grid& g, double k1, double k2) {
   std::vector<int32_t> out;
   for (int i = 0; i < g.nx; ++i)

@@ -74,6 +74,19 @@ struct Rings {
 };
 Rings make_rings(const Grid& g, double dr);
 
+// Azimuthal cells of the FEM correlograph (adfstem.cpp:956-1062,
+// variance.cpp:227-251): n_phi = (ring boundaries in [0.2, 1.0]) - 1 bins of
+// 2 PI / n_phi (PI as the reference's), phi = PI + atan2(ky, kx) per pixel,
+// bin chosen by the reference's loop; pixel lists per (k bin, phi bin) cell
+// [ii * n_phi + jj], each in ring order.
+struct Cells {
+  int32_t n_phi = 0;
+  std::vector<double> phi_bounds;  // n_phi + 1
+  std::vector<int32_t> pix;
+  std::vector<int32_t> start;      // n_k * n_phi + 1 offsets into pix
+};
+Cells make_cells(const Grid& g, const Rings& r);
+
 // Two-dimensional detector MTF before its band limiting (adfstem.cpp:298-384):
 // interleaved complex [nx][ny], real part interpolated from (mtf,
 // domain_sqr) at r^2 = (xpd^2 kx/Nx)^2 + (ypd^2 ky/Ny)^2 and multiplied by

@@ -23,6 +23,7 @@ MSF_FP64, MSF_FP32 = 0, 1
 OUT_ADF_IMAGE = 1 << 0
 OUT_V_OMEGA, OUT_VBAR_R, OUT_V_RE = 1 << 1, 1 << 2, 1 << 3
 OUT_OMEGA_VIMAGE, OUT_V_GT17, OUT_V_RBAR = 1 << 4, 1 << 5, 1 << 6
+OUT_CORRELOGRAPH, OUT_CORRELOGRAPH_VAR = 1 << 7, 1 << 8
 FEM_MODES = {"V_omega": OUT_V_OMEGA, "Vbar_r": OUT_VBAR_R, "V_re": OUT_V_RE,
              "Omega_vimage": OUT_OMEGA_VIMAGE, "V_gt17": OUT_V_GT17,
              "V_rbar": OUT_V_RBAR}
@@ -91,7 +92,10 @@ class Results(C.Structure):
                 ("ring_amplitude", _dp), ("ring_intensity", _dp),
                 ("probe_slices", C.c_int64), ("kernel_launches", C.c_int64),
                 ("seconds_setup", C.c_double),
-                ("seconds_raster", C.c_double)]
+                ("seconds_raster", C.c_double),
+                ("cap_phi", C.c_int32), ("n_phi", C.c_int32), ("phi_lower", _dp),
+                ("correlograph", _dp), ("correlograph_sqr", _dp),
+                ("correlograph_probes", _dp)]
 
 
 class Request(C.Structure):
@@ -306,12 +310,14 @@ class Context:
 
     def run(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
             want_final_psi=False, want_means=False, want_rings=False,
-            cap_k=8192) -> "RunResult":
+            cap_k=8192, want_correlograph_probes=False) -> "RunResult":
         nx, ny = spec.grid.nx, spec.grid.ny
         n_r = raster.n_x * raster.n_y
         if want_rings:
             cap_k = min(cap_k, 1024)
         out = RunResult(n_r, cap_k, nx, ny, want_final_psi, want_means, want_rings)
+        if detect.outputs & OUT_CORRELOGRAPH:
+            out.add_correlograph(spec.grid, detect, n_r, want_correlograph_probes)
         _check(lib().msf_run(self._h, spec._h, C.byref(optics), C.byref(raster),
                              C.byref(detect), C.byref(out._struct)))
         out.finish(raster, detect)
@@ -534,6 +540,26 @@ class RunResult:
         self._struct = s
         self._shape = (nx, ny)
 
+    def add_correlograph(self, grid, detect, n_r, per_probe):
+        """Buffers for the FEM correlograph, sized from the segment counts."""
+        plain = Detect.from_buffer_copy(detect)
+        plain.outputs = (detect.outputs & ~(OUT_CORRELOGRAPH | OUT_CORRELOGRAPH_VAR)) | OUT_V_OMEGA
+        n_k = segment_count(grid, plain) - 1
+        n_phi = (segment_count(grid, detect) - 1 - n_k) // max(n_k, 1)
+        nc = max(1, n_k * n_phi)
+        self.phi_lower = np.zeros(n_phi + 1)
+        self._corr = np.zeros(nc)
+        self._corr_sqr = np.zeros(nc)
+        self._corr_probes = np.zeros(nc * n_r) if per_probe else None
+        s = self._struct
+        s.cap_phi = n_phi
+        s.phi_lower = _p(self.phi_lower)
+        s.correlograph = _p(self._corr)
+        s.correlograph_sqr = _p(self._corr_sqr)
+        if per_probe:
+            s.correlograph_probes = _p(self._corr_probes)
+        self._corr_shape = (n_k, n_phi)
+
     def finish(self, raster, detect):
         s = self._struct
         self.n_k = s.n_k
@@ -544,6 +570,14 @@ class RunResult:
         self.v = {m: self._v[m][:self.n_k] for m in FEM_MODES if detect.outputs & FEM_MODES[m]}
         self.k = self.k_lower[:self.n_k]
         self.counts = self.bin_counts[:self.n_k]
+        if getattr(self, "_corr_shape", None):
+            n_k, n_phi = self._corr_shape
+            # [jj * n_k + ii] -> array [ii (k), jj (phi)]
+            self.correlograph = self._corr[:n_k * n_phi].reshape(n_phi, n_k).T
+            self.correlograph_sqr = self._corr_sqr[:n_k * n_phi].reshape(n_phi, n_k).T
+            if self._corr_probes is not None:
+                self.correlograph_probes = self._corr_probes.reshape(
+                    -1, n_phi, n_k).transpose(0, 2, 1)
         if self.ring_amp is not None:
             self.rings_amp = self.ring_amp.reshape(self._n_r, self._cap_k)[:, :self.n_k]
             self.rings_int = self.ring_int.reshape(self._n_r, self._cap_k)[:, :self.n_k]

@@ -76,6 +76,12 @@ CASES = {
             "--parameter_file mtf.param -m 128 128 200000 --adfstemuncorrfem --V_omega --V_re "
             "--Omega_vimage --cs3 1.3e7 --scherzer_defocus --alphamax 0.010 "
             "--rasterspacing 6.25 --minslice 2.0 --images", True, None),
+    # FEM correlograph: average, variance (squared sums) and every probe's text
+    "corrgraph": (dict(n=780, box=(25, 25, 25), seed=1),
+                  "-m 128 128 200000 --adfstemuncorrfem --V_omega --correlograph "
+                  "--correlograph_variance --correlograph_everytxt --correlograph_everyimage "
+                  "--cs3 1.3e7 --scherzer_defocus --alphamax 0.010 --rasterspacing 6.25 "
+                  "--minslice 2.0 --dr 1.0", True, None),
 }
 
 # extra input files of a case, written beside the specimen (name -> text)
@@ -137,6 +143,12 @@ def run_case(name):
     for f in sorted(work.glob("*_fem_*.txt")):
         mode = f.stem.split("_fem_")[1]
         out[mode] = oracle.read_variance_txt(f)
+    # correlograph tables: first row "0 phi...", then "k values..."
+    for f in sorted(work.glob("*_correlograph_*.txt")):
+        out["correlograph_" + f.stem.split("_correlograph_")[1]] = np.loadtxt(f, ndmin=2)
+    for f in sorted(work.glob(name + "_adfstem_*corr_[0-9]*_[0-9]*.txt")):
+        px, py = f.stem.split("_")[-2:]
+        out["correlograph_probe_%s_%s" % (px, py)] = np.loadtxt(f, ndmin=2)
     sl = np.loadtxt(work / "slices.txt", ndmin=2)
     out["slice_lower"], out["slice_thickness"], out["slice_count"] = sl[:, 0], sl[:, 1], sl[:, 2]
     if tslice is not None:
