@@ -132,7 +132,8 @@ typedef struct {
   double* omega_vimage;
   double* v_gt17;
   double* v_rbar;
-  double* final_psi;       /* 2*nx*ny: last probe's exit wave in k-space      */
+  double* final_psi;       /* 2*nx*ny: last probe's exit wave in k-space (after
+                              the detector MTF when one is applied)          */
   double* mean_amplitude;  /* nx*ny: raster mean of |psi(k)| (FEM pixel modes)*/
   double* mean_intensity;  /* nx*ny: raster mean of |psi(k)|^2                */
   double* ring_amplitude;  /* n_x*n_y*cap_k: per probe, sum |psi| per ring,
@@ -154,6 +155,8 @@ typedef struct {
   double* correlograph;    /* out: raster average                              */
   double* correlograph_sqr;/* out: sum over probes of the squares (variance)   */
   double* correlograph_probes; /* out: n_x*n_y blocks of n_k*n_phi, raster order */
+  double* first_psi;       /* 2*nx*ny: first probe's exit wave in k-space (before
+                              any detector MTF)                               */
 } msf_results;
 
 /* ---- library ---------------------------------------------------------- */

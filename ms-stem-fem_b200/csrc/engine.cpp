@@ -960,6 +960,7 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
     MSF_TRY(ctx->alloc(&stage_int, sizeof(double) * B * n_seg));
   }
   msf_status st = MSF_OK;
+  DevBuf first;
   for (int64_t p0 = 0; p0 < n_probes && st == MSF_OK; p0 += B) {
     const int nb = (int)std::min<int64_t>(B, n_probes - p0);
     if (use_graph && nb == B && p0 > 0) {
@@ -987,12 +988,37 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
       st = enqueue_batch(nb, P.d_shifts.as<int32_t>() + 2 * p0, P.amp.as<double>() + p0 * n_seg,
                          P.inten.as<double>() + p0 * n_seg);
     }
+    if (st == MSF_OK && p0 == 0 && res->first_psi) {
+      // the first probe's exit wave (adfstem.cpp:2139-2221), before the
+      // next batch reuses its buffer
+      MSF_TRY(ctx->alloc(&first, 16 * plane));
+      if (fp64)
+        MSF_CUDA(cudaMemcpyAsync(first.p, psi.p, 16 * plane, cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+      else
+        MSF_CUDA(launch_assemble_split(psi.as<float>(), P.psi0k.as<double>(), g.nx, g.ny,
+                                       P.shifts[0], P.shifts[1], first.as<double>(),
+                                       ctx->stream));
+    }
   }
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (st != MSF_OK) return st;
   MSF_CUDA(cudaEventRecord(ev1, ctx->stream));
 
-  if (res->final_psi) {
+  if (res->first_psi && first.p) {
+    MSF_CUDA(cudaMemcpyAsync(res->first_psi, first.p, 16 * plane, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h_bytes += 16 * plane;
+  }
+  if (res->final_psi && P.mtf) {
+    // the reference's wave after its detector MTF stage (adfstem.cpp:2272-2385)
+    const int last = (int)((n_probes - 1) % B);
+    MSF_CUDA(cudaMemcpyAsync(res->final_psi, mtf_psi.as<double>() + 2 * plane * last, 16 * plane,
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h_bytes += 16 * plane;
+  } else if (res->final_psi) {
     const int last = (int)((n_probes - 1) % B);
     if (fp64) {
       MSF_CUDA(cudaMemcpyAsync(res->final_psi, psi.as<double>() + 2 * plane * last,
@@ -1122,6 +1148,10 @@ msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
       MSF_CUDA(launch_propagate(d, px, px + 2 * g.nx, lo, hi, g.nx, g.ny, st));
       launches += 8;
     }
+    if (p == 0 && res->first_psi) {
+      MSF_CUDA(cudaMemcpy(res->first_psi, d, 16 * plane, cudaMemcpyDeviceToHost));
+      ctx->d2h_bytes += 16 * plane;
+    }
     SplitK none;
     double* amp_p = P.amp.as<double>() + p * P.n_seg;
     double* int_p = P.inten.as<double>() + p * P.n_seg;
@@ -1152,7 +1182,8 @@ msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
   res->probe_slices = P.n_probes * S;
   res->kernel_launches = P.setup_launches + launches;
   if (res->final_psi) {
-    MSF_CUDA(cudaMemcpy(res->final_psi, d, 16 * plane, cudaMemcpyDeviceToHost));
+    MSF_CUDA(cudaMemcpy(res->final_psi, P.mtf ? mtf_psi.as<double>() : d, 16 * plane,
+                        cudaMemcpyDeviceToHost));
     ctx->d2h_bytes += 16 * plane;
   }
   return finish_raster(ctx, P, st, res);

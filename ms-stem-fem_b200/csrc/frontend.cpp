@@ -466,6 +466,91 @@ msf_status read_lammps(const std::string& path, msf_job* j) {
 
 namespace {
 
+// Atomic number of an element symbol (lower case) or of its number written
+// out, 1..103; 0 otherwise (tem_io.cpp:6171-6380).
+unsigned element_z(const std::string& name) {
+  static const char* const symbols[103] = {
+      "h",  "he", "li", "be", "b",  "c",  "n",  "o",  "f",  "ne", "na", "mg", "al", "si", "p",
+      "s",  "cl", "ar", "k",  "ca", "sc", "ti", "v",  "cr", "mn", "fe", "co", "ni", "cu", "zn",
+      "ga", "ge", "as", "se", "br", "kr", "rb", "sr", "y",  "zr", "nb", "mo", "tc", "ru", "rh",
+      "pd", "ag", "cd", "in", "sn", "sb", "te", "i",  "xe", "cs", "ba", "la", "ce", "pr", "nd",
+      "pm", "sm", "eu", "gd", "tb", "dy", "ho", "er", "tm", "yb", "lu", "hf", "ta", "w",  "re",
+      "os", "ir", "pt", "au", "hg", "tl", "pb", "bi", "po", "at", "rn", "fr", "ra", "ac", "th",
+      "pa", "u",  "np", "pu", "am", "cm", "bk", "cf", "es", "fm", "md", "no", "lr"};
+  for (unsigned z = 1; z <= 103; ++z)
+    if (name == symbols[z - 1] || name == std::to_string(z)) return z;
+  return 0;
+}
+
+}  // namespace
+
+// read_position_xyz_file (tem_io.cpp:4627-4958): atom count, then the three
+// periods, then one "element x y z" line per atom (each line followed by a
+// newline).  Coordinates are shifted by the smallest value of each axis,
+// which starts at 0 (so only negative coordinates move); a spread larger
+// than the period is an error.
+msf_status read_xyz(const std::string& path, msf_job* j) {
+  std::ifstream in(path.c_str());
+  if (!in.is_open()) {
+    j->messages += "Error opening position file: " + path + "\n";
+    return MSF_ERR_IO;
+  }
+  auto fail = [&](const std::string& m) {
+    j->messages += "Error reading position data file; " + m + "\n";
+    return MSF_ERR_PARSE;
+  };
+  std::string line;
+  size_t declared = 0;
+  if (!(std::getline(in, line) && in.good())) return fail("data_line : " + line);
+  {
+    std::istringstream ls(line);
+    ls >> declared;
+    if (!declared) return fail("declared_population : 0");
+  }
+  if (!(std::getline(in, line) && in.good())) return fail("data_line : " + line);
+  {
+    std::istringstream ls(line);
+    double px = 0, py = 0, pz = 0;
+    ls >> px >> py >> pz;
+    if (!(px > 0.0 && py > 0.0 && pz > 0.0))
+      return fail("second line should begin with <xperiod> <yperiod> <zperiod>");
+    j->xperiod = px;
+    j->yperiod = py;
+    j->zperiod = pz;
+  }
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  j->q.clear();
+  j->z.clear();
+  for (size_t n = 0; n < declared; ++n) {
+    if (!(std::getline(in, line) && in.good()))
+      return fail("atoms read : " + std::to_string(n) + ", declared population : " +
+                  std::to_string(declared));
+    std::istringstream ls(line);
+    std::string element;
+    ls >> element;
+    element = lower(element);
+    const unsigned zz = element_z(element);
+    if (zz < 1 || zz > 103)
+      return fail("atom " + std::to_string(n) + ", element " + element + " invalid");
+    double q[3] = {0, 0, 0};
+    ls >> q[0] >> q[1] >> q[2];
+    for (int d = 0; d < 3; ++d) {
+      if (q[d] < lo[d]) lo[d] = q[d];
+      if (q[d] > hi[d]) hi[d] = q[d];
+      j->q.push_back(q[d]);
+    }
+    j->z.push_back(zz);
+  }
+  if (hi[0] - lo[0] > j->xperiod || hi[1] - lo[1] > j->yperiod || hi[2] - lo[2] > j->zperiod)
+    return fail("positions exceed period");
+  for (size_t a = 0; a < j->z.size(); ++a)
+    for (int d = 0; d < 3; ++d) j->q[3 * a + d] = j->q[3 * a + d] - lo[d];
+  j->xmin = j->ymin = j->zmin = 0.0;
+  return MSF_OK;
+}
+
+namespace {
+
 // tem.cpp:405-1378 after the inputs are read
 msf_status finish_job(msf_job* j) {
   Flags& f = j->flags;
@@ -618,12 +703,10 @@ msf_status msf_read_specimen(const char* path, msf_job** out) {
   msf_job* j = new msf_job;
   const std::string p(path);
   msf_status st;
-  if (p.size() > 4 && p.substr(p.find_last_of('.') + 1) == "xyz") {
-    j->messages += "Error, xyz specimen files are not supported by this build\n";
-    st = MSF_ERR_UNSUPPORTED;
-  } else {
+  if (p.substr(p.find_last_of('.') + 1) == "xyz")  // tem.cpp:288-330
+    st = read_xyz(p, j);
+  else
     st = read_lammps(p, j);
-  }
   if (st != MSF_OK) {
     msf::set_error(j->messages);
     delete j;
@@ -641,12 +724,8 @@ msf_status msf_parse_cmdline(int32_t argc, const char* const* argv, msf_job** ou
   parse_args(args, j);
   // tem.cpp:240-330: the specimen is read before the flag checks
   msf_status st = MSF_OK;
-  if (!j->model_file.empty() &&
-      j->model_file.substr(j->model_file.find_last_of('.') + 1) == "xyz") {
-    j->messages += "Error, xyz specimen files are not supported by this build\n";
-    j->flags.fail = 1;
-    st = MSF_ERR_UNSUPPORTED;
-  } else if (read_lammps(j->model_file, j) != MSF_OK) {
+  const bool xyz = j->model_file.substr(j->model_file.find_last_of('.') + 1) == "xyz";
+  if ((xyz ? read_xyz(j->model_file, j) : read_lammps(j->model_file, j)) != MSF_OK) {
     j->messages += "Error, file could not be read : " + j->model_file + "\n";
     j->flags.fail = 1;
     st = MSF_ERR_IO;
@@ -814,6 +893,42 @@ msf_status msf_write_outputs(const msf_job* j, const msf_results* r) {
       return MSF_ERR_IO;
     }
   }
+  if (f.image_output) {
+    // output_diffraction (write_tif.cpp:817-1098): log(1 + s |psi|^2),
+    // quadrants swapped, min/max scaled, rows bottom-up; resolution
+    // xperiod_duped * 1e-8, unit none; the scale factor in the file name is
+    // printed by an ostringstream.  The first probe at five scales
+    // (adfstem.cpp:2139-2221), the last one at scale 1 (:3778-3799).
+    const size_t nx = (size_t)j->nx, ny = (size_t)j->ny;
+    const double xres = j->xperiod * j->dupe_x * 1.0e-8, yres = j->yperiod * j->dupe_y * 1.0e-8;
+    auto diffraction = [&](const double* psi, double scale, const std::string& tag) {
+      std::vector<double> m(nx * ny);
+      for (size_t k = 0; k < nx * ny; ++k) {
+        const double re = psi[2 * k], im = psi[2 * k + 1];
+        m[k] = std::log(1.0 + (scale * (re * re + im * im)));
+      }
+      double mn = m[0], mx = m[0];
+      for (size_t k = 1; k < nx * ny; ++k) { mx = std::max(mx, m[k]); mn = std::min(mn, m[k]); }
+      for (size_t i = 0; i < nx / 2; ++i) {
+        for (size_t k = 0; k < ny / 2; ++k)
+          std::swap(m[k + i * ny], m[(k + ny / 2) + (i + nx / 2) * ny]);
+        for (size_t k = ny / 2; k < ny; ++k)
+          std::swap(m[k + i * ny], m[(k - ny / 2) + (i + nx / 2) * ny]);
+      }
+      std::ostringstream sf;
+      sf << scale;
+      const std::string name = pre + tag + "_diffraction_scalefactor_" + sf.str() + ".tif";
+      if (!write_tif16(name, m.data(), nx, ny, mn, mx, false, xres, yres, 1)) {
+        msf::set_error("could not write " + name);
+        return false;
+      }
+      return true;
+    };
+    if (r->first_psi)
+      for (double scale : {1.0e-5, 1.0e-1, 1.0e0, 1.0e10, 1.0e+20})
+        if (!diffraction(r->first_psi, scale, "_first")) return MSF_ERR_IO;
+    if (r->final_psi && !diffraction(r->final_psi, 1.0e+0, "_final")) return MSF_ERR_IO;
+  }
   if (f.image_output && r->adf_image) {
     const size_t nx = j->x_p.size(), ny = j->y_p.size();
     const double* img = r->adf_image;
@@ -888,6 +1003,13 @@ int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) 
         corr_probes.assign(nc * nr, 0.0);
         r.correlograph_probes = corr_probes.data();
       }
+    }
+    std::vector<double> final_psi, first_psi;
+    if (j->flags.image_output) {  // the first and last exit waves' diffraction
+      final_psi.assign(2 * (size_t)grid.nx * grid.ny, 0.0);
+      first_psi.assign(2 * (size_t)grid.nx * grid.ny, 0.0);
+      r.final_psi = final_psi.data();
+      r.first_psi = first_psi.data();
     }
     if ((st = msf_run(ctx, spec, &optics, &raster, &det, &r)) == MSF_OK &&
         (st = msf_write_outputs(j, &r)) == MSF_OK)

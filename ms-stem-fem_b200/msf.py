@@ -95,7 +95,7 @@ class Results(C.Structure):
                 ("seconds_raster", C.c_double),
                 ("cap_phi", C.c_int32), ("n_phi", C.c_int32), ("phi_lower", _dp),
                 ("correlograph", _dp), ("correlograph_sqr", _dp),
-                ("correlograph_probes", _dp)]
+                ("correlograph_probes", _dp), ("first_psi", _dp)]
 
 
 class Request(C.Structure):
@@ -516,6 +516,7 @@ class RunResult:
         self.bin_counts = np.zeros(cap_k, dtype=np.int32)
         self._v = {m: np.full(cap_k, np.nan) for m in FEM_MODES}
         self.final_psi = np.zeros(2 * nx * ny) if want_psi else None
+        self.first_psi = np.zeros(2 * nx * ny) if want_psi else None
         self.mean_amplitude = np.zeros(nx * ny) if want_means else None
         self.mean_intensity = np.zeros(nx * ny) if want_means else None
         s = Results()
@@ -527,6 +528,7 @@ class RunResult:
             setattr(s, f, _p(self._v[m]))
         if want_psi:
             s.final_psi = _p(self.final_psi)
+            s.first_psi = _p(self.first_psi)
         if want_means:
             s.mean_amplitude = _p(self.mean_amplitude)
             s.mean_intensity = _p(self.mean_intensity)

@@ -253,6 +253,25 @@ def read_lammps(path):
     return np.array(q), np.array(z, dtype=np.uint32), [h - l for h, l in zip(hi, lo)]
 
 
+def read_xyz(path):
+    """Minimal reader of the xyz grammar (tem_io.cpp:4627-4958) for the
+    oracle: count, periods, then element and position per line (symbols of
+    the golden cases: Si in any case, or 14); positions shifted by their
+    minimum taken from 0."""
+    lines = Path(path).read_text().splitlines()
+    n = int(lines[0].split()[0])
+    per = [float(v) for v in lines[1].split()[:3]]
+    q, z = [], []
+    for line in lines[2:2 + n]:
+        p = line.split()
+        assert p[0].lower() in ("si", "14")
+        q.append([float(v) for v in p[1:4]])
+        z.append(14)
+    q = np.array(q)
+    q = q - np.minimum(q.min(axis=0), 0.0)
+    return q, np.array(z, dtype=np.uint32), per
+
+
 def job_from_argv(argv, cwd):
     """The oracle's own derivation of tem.cpp:405-1378 for an argv (the option
     subset the golden cases use).  Returns (job dict, q, z)."""
@@ -275,7 +294,8 @@ def job_from_argv(argv, cwd):
         else:
             flags.add(k)
             i += 1
-    q, z, per = read_lammps(Path(cwd) / opt["-a"])
+    spec = Path(cwd) / opt["-a"]
+    q, z, per = read_xyz(spec) if spec.suffix == ".xyz" else read_lammps(spec)
     nx, ny, vv = int(opt["-m"][0]), int(opt["-m"][1]), float(opt["-m"][2])
     lam = C.c_double()
     gam = C.c_double()

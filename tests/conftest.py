@@ -42,7 +42,7 @@ def case_dir(name, tmp_root: Path) -> Path:
     d.mkdir(parents=True, exist_ok=True)
     target = d / meta["argv"][1]
     if meta["committed_specimen"]:
-        shutil.copy(GOLDEN / (name + ".data"), target)
+        shutil.copy(GOLDEN / meta["argv"][1], target)
     else:
         if name not in _SPEC_CACHE:
             sys.path.insert(0, str(GOLDEN))

@@ -30,6 +30,7 @@ sys.path.insert(0, str(ROOT / "ms-stem-fem_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
 import specimen  # noqa: E402
 import oracle  # noqa: E402
+from tif16 import read_tif16  # noqa: E402
 
 FEM_ALL = ["--V_omega", "--Vbar_r", "--V_re", "--Omega_vimage", "--V_gt17", "--V_rbar"]
 
@@ -76,6 +77,10 @@ CASES = {
             "--parameter_file mtf.param -m 128 128 200000 --adfstemuncorrfem --V_omega --V_re "
             "--Omega_vimage --cs3 1.3e7 --scherzer_defocus --alphamax 0.010 "
             "--rasterspacing 6.25 --minslice 2.0 --images", True, None),
+    # xyz specimen file (element symbols in any case, or the atomic number)
+    "xyz": (dict(n=780, box=(25, 25, 25), seed=3, xyz=True),
+            "-m 128 128 200000 --adfstemuncorrfem --V_omega --cs3 1.3e7 --scherzer_defocus "
+            "--alphamax 0.010 --rasterspacing 6.25 --minslice 2.0 --images", True, None),
     # FEM correlograph: average, variance (squared sums) and every probe's text
     "corrgraph": (dict(n=780, box=(25, 25, 25), seed=1),
                   "-m 128 128 200000 --adfstemuncorrfem --V_omega --correlograph "
@@ -91,7 +96,22 @@ FILES = {
 }
 
 
+def write_xyz(path, pos, box):
+    """xyz specimen (tem_io.cpp:4627-4958): count, periods, then element and
+    position per line; element names in mixed case and as a number."""
+    names = ["Si", "si", "SI", "14"]
+    lines = ["%d" % len(pos), "%.6f %.6f %.6f" % tuple(box)]
+    for k, p in enumerate(pos):
+        lines.append("%s %.6f %.6f %.6f" % (names[k % 4], p[0], p[1], p[2]))
+    Path(path).write_text("\n".join(lines) + "\n")
+
+
 def make_specimen_file(recipe, path):
+    if recipe.get("xyz"):
+        pos = specimen.amorphous_positions(recipe["n"], recipe["box"], seed=recipe["seed"])
+        pos = np.minimum(np.round(pos, 6), np.round(np.asarray(recipe["box"], float), 6))
+        write_xyz(path, pos, recipe["box"])
+        return pos
     pos = specimen.make_specimen(path, recipe["n"], recipe["box"], seed=recipe["seed"])
     if recipe.get("two_species"):
         # every third atom becomes oxygen (mass 15.999 -> Z = 8)
@@ -122,7 +142,7 @@ def sha256(path):
 def run_case(name):
     recipe, args, commit, tslice = CASES[name]
     work = Path(tempfile.mkdtemp(prefix="golden_" + name))
-    spec = work / (name + ".data")
+    spec = work / (name + (".xyz" if recipe.get("xyz") else ".data"))
     make_specimen_file(recipe, spec)
     for fname, text in FILES.get(name, {}).items():
         (work / fname).write_text(text)
@@ -149,6 +169,9 @@ def run_case(name):
     for f in sorted(work.glob(name + "_adfstem_*corr_[0-9]*_[0-9]*.txt")):
         px, py = f.stem.split("_")[-2:]
         out["correlograph_probe_%s_%s" % (px, py)] = np.loadtxt(f, ndmin=2)
+    for tag in ("first", "final"):  # diffraction patterns written with --images
+        for f in work.glob("*_%s_diffraction_scalefactor_*.tif" % tag):
+            out["%s_diffraction_%s" % (tag, f.stem.split("_scalefactor_")[1])] = read_tif16(f)
     sl = np.loadtxt(work / "slices.txt", ndmin=2)
     out["slice_lower"], out["slice_thickness"], out["slice_count"] = sl[:, 0], sl[:, 1], sl[:, 2]
     if tslice is not None:
@@ -161,7 +184,7 @@ def run_case(name):
                 adfstem_seconds=r["adfstem_seconds"], probes=r["probes"], slices=r["slices"])
     (HERE / (name + ".json")).write_text(json.dumps(meta, indent=1) + "\n")
     if commit:
-        shutil.copy(spec, HERE / (name + ".data"))
+        shutil.copy(spec, HERE / spec.name)
     shutil.rmtree(work)
     print(name, "ok", r["adfstem_seconds"], "s", sorted(out))
 

@@ -7,7 +7,7 @@ import pytest
 import oracle
 from conftest import assert_variance_close, case_dir, load_case, rel_err
 
-SMALL = ["fem128", "corr", "rect", "sio", "dupe", "c1"]
+SMALL = ["fem128", "corr", "rect", "sio", "dupe", "c1", "xyz"]
 
 
 @pytest.mark.parametrize("name", SMALL)
