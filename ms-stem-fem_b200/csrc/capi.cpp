@@ -78,6 +78,8 @@ msf_status msf_context_create(const msf_options* opt, msf_context** out) {
   c->batch = o.batch;
   c->graphs = o.use_graphs != 0;
   if (const char* p = std::getenv("MSF_PIPE")) c->pipe = std::atoi(p);
+  if (const char* p = std::getenv("MSF_POTENTIAL"))
+    c->potential = std::string(p) == "direct" ? 1 : std::string(p) == "fft" ? 2 : 0;
   c->budget = o.hbm_budget;
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {

@@ -142,6 +142,10 @@ msf_status fft2d_f64(msf_context* ctx, const Grid& g, double* planes, int nb, bo
 
 bool grid_ok(int n) { return supported_length(n); }
 
+// slices with at least this many atoms take the FFT convolution for their
+// potential (about the atom count at which it costs less than the direct sum)
+constexpr int64_t kPotentialFftAtoms = 64;
+
 }  // namespace
 
 msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms* atoms,
@@ -198,7 +202,7 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
   MSF_TRY(upload(ctx, &spec->ky, g.ky));
 
   // per-species LUTs (scatterer_pap.hpp:109-190)
-  DevBuf luts, params;
+  DevBuf luts, luts_k, params;
   MSF_TRY(ctx->alloc(&luts, sizeof(double) * 2 * plane * std::max<size_t>(1, species.size())));
   std::vector<double> hp;
   for (uint32_t z : species) hp.insert(hp.end(), kirkland_params(z), kirkland_params(z) + 12);
@@ -210,12 +214,23 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
                               spec->ky.as<double>(), g.nx, g.ny, params.as<double>() + 12 * k,
                               pref, g.bw_pap * g.bw_pap, g.xmin, g.ymin, ctx->stream));
   }
+  // slicing (slice.cpp:469-980) and per-atom pixel snaps (slice.cpp:1556-1572)
+  Slicing sl = slice_atoms(n, q.data(), g.zmin, g.zpd, gin->min_slice);
+  // which slices take the FFT convolution for their potential
+  std::vector<uint8_t> by_fft(sl.n(), 0);
+  for (int64_t s = 0; s < sl.n(); ++s) {
+    const int64_t cnt = sl.start[s + 1] - sl.start[s];
+    by_fft[s] = ctx->potential == 2 || (ctx->potential == 0 && cnt >= kPotentialFftAtoms);
+  }
+  const bool any_fft = std::find(by_fft.begin(), by_fft.end(), 1) != by_fft.end();
+  if (any_fft && !species.empty()) {  // keep the k-space LUTs
+    MSF_TRY(ctx->alloc(&luts_k, luts.bytes));
+    MSF_CUDA(cudaMemcpyAsync(luts_k.p, luts.p, luts.bytes, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+  }
   if (!species.empty())
     MSF_TRY(fft2d_f64(ctx, g, luts.as<double>(), (int)species.size(), true,
                       1.0 / std::sqrt((double)(g.nx * (int64_t)g.ny))));
-
-  // slicing (slice.cpp:469-980) and per-atom pixel snaps (slice.cpp:1556-1572)
-  Slicing sl = slice_atoms(n, q.data(), g.zmin, g.zpd, gin->min_slice);
   spec->n_slices = (int)sl.n();
   spec->lower = sl.lower;
   spec->thickness = sl.thickness;
@@ -239,6 +254,34 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
   MSF_TRY(upload(ctx, &dsx, asx));
   MSF_TRY(upload(ctx, &dsy, asy));
   MSF_TRY(upload(ctx, &dsp, asp));
+  // pixel histograms of the FFT slices: (species, pixel, count) runs
+  std::vector<int32_t> h_pix, h_sp;
+  std::vector<double> h_cnt;
+  std::vector<int64_t> h_start(sl.n() + 1, 0);
+  for (int64_t s = 0; s < sl.n(); ++s) {
+    if (by_fft[s]) {
+      std::vector<int64_t> keys;
+      for (int64_t k = sl.start[s]; k < sl.start[s + 1]; ++k)
+        keys.push_back(((int64_t)asp[k] * g.nx + asx[k]) * g.ny + asy[k]);
+      std::sort(keys.begin(), keys.end());
+      for (size_t k = 0; k < keys.size();) {
+        size_t e = k;
+        while (e < keys.size() && keys[e] == keys[k]) ++e;
+        h_sp.push_back((int32_t)(keys[k] / plane));
+        h_pix.push_back((int32_t)(keys[k] % plane));
+        h_cnt.push_back((double)(e - k));
+        k = e;
+      }
+    }
+    h_start[s + 1] = (int64_t)h_pix.size();
+  }
+  DevBuf d_hpix, d_hsp, d_hcnt, hist;
+  if (any_fft) {
+    MSF_TRY(upload(ctx, &d_hpix, h_pix));
+    MSF_TRY(upload(ctx, &d_hsp, h_sp));
+    MSF_TRY(upload(ctx, &d_hcnt, h_cnt));
+    MSF_TRY(ctx->alloc(&hist, 16 * plane * std::max<size_t>(1, species.size())));
+  }
 
   // band-limit mask (shared by the transmission build and the propagator)
   std::vector<int32_t> lo, hi;
@@ -264,9 +307,24 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
   for (int64_t s = 0; s < sl.n(); ++s) {
     double* t64 = ctx->fp64 ? spec->t.as<double>() + 2 * plane * s : scratch.as<double>();
     const int64_t s0 = sl.start[s], cnt = sl.start[s + 1] - sl.start[s];
-    MSF_CUDA(launch_potential(t64, luts.as<double>(), g.nx, g.ny, dsx.as<int32_t>() + s0,
-                              dsy.as<int32_t>() + s0, dsp.as<int32_t>() + s0, (int)cnt,
-                              ctx->stream));
+    if (by_fft[s] && !species.empty()) {
+      // BACKWARD(lut_k * FORWARD(H)) / s, then the exponential
+      MSF_CUDA(cudaMemsetAsync(hist.p, 0, hist.bytes, ctx->stream));
+      MSF_CUDA(launch_histogram_scatter(hist.as<double>(), d_hpix.as<int32_t>() + h_start[s],
+                                        d_hsp.as<int32_t>() + h_start[s],
+                                        d_hcnt.as<double>() + h_start[s],
+                                        (int)(h_start[s + 1] - h_start[s]), plane, ctx->stream));
+      MSF_TRY(fft2d_f64(ctx, g, hist.as<double>(), (int)species.size(), false, 1.0));
+      MSF_CUDA(launch_histogram_lut(t64, hist.as<double>(), luts_k.as<double>(),
+                                    (int)species.size(), plane, ctx->stream));
+      MSF_TRY(fft2d_f64(ctx, g, t64, 1, true, 1.0));
+      MSF_CUDA(launch_transmission_exp(t64, plane, 1.0 / std::sqrt((double)(g.nx * (int64_t)g.ny)),
+                                       ctx->stream));
+    } else {
+      MSF_CUDA(launch_potential(t64, luts.as<double>(), g.nx, g.ny, dsx.as<int32_t>() + s0,
+                                dsy.as<int32_t>() + s0, dsp.as<int32_t>() + s0, (int)cnt,
+                                ctx->stream));
+    }
     a.psi = t64;
     MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
     MSF_CUDA(launch_row(true, ROW_FWD, a, ctx->stream));

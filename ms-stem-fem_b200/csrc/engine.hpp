@@ -47,6 +47,10 @@ struct msf_context {
   // persistent TMA-pipelined FP32 passes: bit mask of MSF_PIPE_COL and
   // MSF_PIPE_ROW, overridden by the MSF_PIPE environment variable
   int pipe = MSF_PIPE_COL;
+  // slice potentials: 0 FFT convolution for slices of at least 64 atoms,
+  // direct sum otherwise; 1 always direct; 2 always FFT (MSF_POTENTIAL =
+  // direct / fft)
+  int potential = 0;
   int64_t budget = 0;
   int64_t allocated = 0;
   int64_t h2d_bytes = 0, d2h_bytes = 0;

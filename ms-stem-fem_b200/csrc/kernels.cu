@@ -423,6 +423,46 @@ __global__ void potential_kernel(double2* __restrict__ t, const double2* __restr
   }
 }
 
+// ---- potential by FFT convolution -------------------------------------
+// The slice's sum over atoms of the LUT shifted to each atom's pixel is the
+// circular convolution of the pixel histogram H with the LUT; with the LUT
+// defined as BACKWARD(lut_k) / s (scatterer_pap.hpp:86-190) it equals
+// BACKWARD(lut_k * FORWARD(H)) / s.
+// H[sp][pix] = count for the slice's (species, pixel) pairs (unique pixels).
+__global__ void histogram_scatter_kernel(double2* __restrict__ h, const int32_t* __restrict__ pix,
+                                         const int32_t* __restrict__ sp,
+                                         const double* __restrict__ count, int n,
+                                         int64_t plane) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) h[(int64_t)sp[k] * plane + pix[k]] = make_double2(count[k], 0.0);
+}
+
+// out = sum over species of H_s * lut_s (k-space, FP64)
+__global__ void histogram_lut_kernel(double2* __restrict__ out, const double2* __restrict__ h,
+                                     const double2* __restrict__ lut_k, int n_species,
+                                     int64_t plane) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= plane) return;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int s = 0; s < n_species; ++s) {
+    const double2 a = h[(int64_t)s * plane + p], b = lut_k[(int64_t)s * plane + p];
+    acc.x += a.x * b.x - a.y * b.y;
+    acc.y += a.x * b.y + a.y * b.x;
+  }
+  out[p] = acc;
+}
+
+// t = e^{-Im v} (cos Re v, sin Re v) with v = t * scale (slice.cpp:1700-1725)
+__global__ void transmission_exp_kernel(double2* __restrict__ t, int64_t n, double scale) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double re = t[k].x * scale, im = t[k].y * scale;
+  const double e = exp(-(im));
+  double sn, cs;
+  sincos(re, &sn, &cs);
+  t[k] = make_double2(e * cs, e * sn);
+}
+
 __global__ void probe_synth_kernel(double2* out, const double* __restrict__ kx,
                                    const double* __restrict__ ky, int nx, int ny,
                                    int corrected, double cs3, double cs5,
@@ -898,6 +938,28 @@ cudaError_t launch_segment_sums(bool fp64, const void* psi, int64_t stride, int 
     if (e != cudaSuccess) return e;
   }
   segment_reduce_kernel<<<nb, 128, 0, s>>>(pa, pi, sp.seg_chunk, sp.ng, sp.n_chunks, amp, inten);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_histogram_scatter(double* h, const int32_t* pix, const int32_t* sp,
+                                     const double* count, int n, int64_t plane, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  histogram_scatter_kernel<<<blocks_for(n, 256), 256, 0, s>>>(reinterpret_cast<double2*>(h), pix,
+                                                              sp, count, n, plane);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_histogram_lut(double* out, const double* h, const double* lut_k,
+                                 int n_species, int64_t plane, cudaStream_t s) {
+  histogram_lut_kernel<<<blocks_for(plane, 256), 256, 0, s>>>(
+      reinterpret_cast<double2*>(out), reinterpret_cast<const double2*>(h),
+      reinterpret_cast<const double2*>(lut_k), n_species, plane);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transmission_exp(double* t, int64_t n, double scale, cudaStream_t s) {
+  transmission_exp_kernel<<<blocks_for(n, 256), 256, 0, s>>>(reinterpret_cast<double2*>(t), n,
+                                                             scale);
   return cudaGetLastError();
 }
 

@@ -121,6 +121,14 @@ cudaError_t launch_potential(double* t, const double* luts, int nx, int ny,
                              const int32_t* atom_sx, const int32_t* atom_sy,
                              const int32_t* atom_species, int n_atoms,
                              cudaStream_t s);
+// Potential by FFT convolution (the direct sum's exact equivalent):
+// H[sp[k]][pix[k]] = count[k] on zeroed planes; out = sum_s H_s * lut_s in
+// k-space; t = e^{-Im v} (cos Re v, sin Re v) with v = t * scale.
+cudaError_t launch_histogram_scatter(double* h, const int32_t* pix, const int32_t* sp,
+                                     const double* count, int n, int64_t plane, cudaStream_t s);
+cudaError_t launch_histogram_lut(double* out, const double* h, const double* lut_k,
+                                 int n_species, int64_t plane, cudaStream_t s);
+cudaError_t launch_transmission_exp(double* t, int64_t n, double scale, cudaStream_t s);
 // Probe in k-space before the inverse transform (probe_wavefunction.cpp).
 cudaError_t launch_probe_synth(double* out, const double* kx, const double* ky,
                                int nx, int ny, int corrected, double cs3,
