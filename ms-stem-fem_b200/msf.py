@@ -18,6 +18,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libmsf.so"
 CLI_PATH = HERE / "bin" / "ms-stem-fem"
+ABI_VERSION = 2  # MSF_ABI_VERSION of the include/msf.h these structs mirror
 
 MSF_FP64, MSF_FP32 = 0, 1
 OUT_ADF_IMAGE = 1 << 0
@@ -184,6 +185,9 @@ def lib() -> C.CDLL:
         L.msf_probe_noalloc.argtypes = [C.POINTER(Grid), C.POINTER(Optics), C.c_void_p,
                                         C.c_void_p]
         L.msf_time_passes.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]
+        if L.msf_abi_version() != ABI_VERSION:
+            raise RuntimeError("libmsf.so has ABI version %d, these bindings expect %d: "
+                               "rebuild it" % (L.msf_abi_version(), ABI_VERSION))
         _lib = L
     return _lib
 

@@ -25,7 +25,9 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) == set(msf.EXPORTED)
-    assert lib.msf_abi_version() == 2
+    header = (ROOT / "include" / "msf.h").read_text()
+    abi = int(re.search(r"#define MSF_ABI_VERSION (\d+)", header).group(1))
+    assert lib.msf_abi_version() == abi == msf.ABI_VERSION
 
 
 @pytest.mark.parametrize("name", golden_cases())
