@@ -40,6 +40,24 @@ template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) 
   return C{a.x * s, a.y * s};
 }
 
+// FP32 complex adds and scales on the paired FP32 pipe of sm_100 (one
+// FADD2 / FMUL2 per complex operation), with the same per-component
+// round-to-nearest results as the scalar operations.
+#ifndef MSF_FP32X2
+#define MSF_FP32X2 1
+#endif
+#if MSF_FP32X2 && defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+  return __fadd2_rn(a, b);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
+template <> __device__ __forceinline__ float2 cscale<float2, float>(float2 a, float s) {
+  return __fmul2_rn(a, make_float2(s, s));
+}
+#endif
+
 template <int I> using ic = std::integral_constant<int, I>;
 
 // Loads issued between two fences may be scheduled together; a fence keeps

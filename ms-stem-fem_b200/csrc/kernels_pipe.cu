@@ -256,7 +256,9 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
       C v[E];
 #pragma unroll
       for (int m = 0; m < E; ++m) v[m] = base[(t + T * m) * COLS + c];
-      __syncthreads();
+      // the transform's first exchange opens with a barrier, which also
+      // orders these tile reads before its writes into the same buffer
+      if constexpr (Sh::S == 1) __syncthreads();
       C* sm = base + c * SM::stride;
       fft_line<Sh, false>(v, sm, t, tw, sync);
       const int lo = __ldg(mask_lo + j), hi = __ldg(mask_hi + j);
