@@ -217,6 +217,24 @@ msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
 msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
                              double* probe_device, void* stream);
 
+/* ---- MD-coupled FEM (the reference's ms-stem-fem-md) -------------------- */
+/* Replaces the raster loop of ftem_lammps.cpp main (1513-3610, 4077-4990):
+ * every probe position is propagated through `samples` configurations of
+ * the specimen, sample s through snapshots[s % n_snapshots] (samples must
+ * be a multiple of n_snapshots); its exit waves (after the detector MTF
+ * when one is given) are averaged coherently, psi_acc += psi / samples
+ * (:3601-3610), the ADF image is the average of the samples' ADF signals
+ * (:3385-3402), and the FEM statistics, correlograph and pixel means are
+ * those of msf_run evaluated on psi_acc (:3686-3990).  The snapshots must
+ * share the grid, voltage and lateral cell (x/y periods, duplication and
+ * minima); their z extents, atoms and slicing may differ.  final_psi gets
+ * the last probe's psi_acc; first_psi is not filled.  probe_slices counts
+ * every propagation of every sample. */
+msf_status msf_run_md(msf_context* ctx, int32_t n_snapshots,
+                      const msf_specimen* const* snapshots, int32_t samples,
+                      const msf_optics* optics, const msf_raster* raster,
+                      const msf_detect* detect, msf_results* results);
+
 /* ---- one raster sharded over several GPUs ------------------------------ */
 /* The reference splits a raster over MPI ranks and reduces the detector
  * sums with MPI_Reduce / MPI_Allgatherv (adfstem.cpp:1556-1606, 2489-2782,
@@ -365,6 +383,17 @@ msf_status msf_write_outputs(const msf_job* job, const msf_results* res);
  * exit status the reference would return (0 success, 1 failure). */
 int32_t msf_main(int32_t argc, const char* const* argv,
                  const msf_options* opt);
+/* The drop-in ms-stem-fem-md program (ftem_lammps.cpp main), argv as the
+ * reference's, with LAMMPS replaced by a replay of LAMMPS data files: the
+ * pre-TEM file's read_data gives the initial configuration (and the cell),
+ * its tersoff / sw / eam pair_coeff line the element of each atom type, and
+ * the i-th "run" of the MD loads entry (i - 1) mod K of the list that
+ * `--md_replay <file>` names (one data file per line; with
+ * --lammps_TEM_steps 0 nothing runs and every sample sees the initial
+ * configuration).  lammps_TEM_samples must be a multiple of K.  Outputs go
+ * under the plain output prefix, as there. */
+int32_t msf_md_main(int32_t argc, const char* const* argv,
+                    const msf_options* opt);
 
 #ifdef __cplusplus
 }

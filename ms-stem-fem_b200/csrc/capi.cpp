@@ -195,6 +195,17 @@ msf_status msf_run(msf_context* ctx, const msf_specimen* spec, const msf_optics*
   return run_raster(ctx, spec, optics, raster, detect, results);
 }
 
+msf_status msf_run_md(msf_context* ctx, int32_t n_snapshots,
+                      const msf_specimen* const* snapshots, int32_t samples,
+                      const msf_optics* optics, const msf_raster* raster,
+                      const msf_detect* detect, msf_results* results) {
+  if (!ctx) {
+    set_error("null context");
+    return MSF_ERR_ARG;
+  }
+  return run_md(ctx, n_snapshots, snapshots, samples, optics, raster, detect, results);
+}
+
 msf_status msf_run_plain(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                          const msf_raster* raster, const msf_detect* detect,
                          msf_results* results) {

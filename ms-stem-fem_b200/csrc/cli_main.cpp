@@ -1,7 +1,10 @@
 // ms-stem-fem: drop-in replacement for the reference executable's ADF-STEM /
-// FEM path (tem.cpp:81-1771).  Accepts the reference's options and
-// parameter files unchanged; three options of this build are taken out
-// before the reference's parser sees the rest, and none changes a default:
+// FEM path (tem.cpp:81-1771); built with MSF_MD_DRIVER it is ms-stem-fem-md,
+// the replacement of the LAMMPS-coupled driver (ftem_lammps.cpp), which also
+// takes --md_replay <file> (msf_md_main in msf.h).  Accepts the reference's
+// options and parameter files unchanged; three options of this build are
+// taken out before the reference's parser sees the rest, and none changes a
+// default:
 //   --precision fp64|fp32   wavefield/FFT precision (default fp64, as the
 //                           reference)
 //   --batch <n>             probes per launch (default: from free memory)
@@ -35,5 +38,9 @@ int main(int argc, char** argv) {
       rest.push_back(argv[i]);
     }
   }
+#ifdef MSF_MD_DRIVER
+  return msf_md_main((int32_t)rest.size(), rest.data(), &opt);
+#else
   return msf_main((int32_t)rest.size(), rest.data(), &opt);
+#endif
 }

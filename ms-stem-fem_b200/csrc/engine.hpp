@@ -155,4 +155,14 @@ msf_status run_batch(msf_context* ctx, int n, const msf_specimen* const* specs,
                      const msf_optics* optics, const msf_raster* rasters,
                      const msf_detect* detects, msf_results* results, int slots);
 int lane_slots(int want, int64_t plane, int lanes, int64_t probes);
+struct SplitK;
+// The detector MTF stage of nb exit waves into FP64 planes `out` (the plan
+// supplies the grid, aperture and the 2-D MTF).
+msf_status mtf_stage(msf_context* ctx, const RasterPlan& P, bool fp64, const void* psi, int nb,
+                     const SplitK& sk, double* out, cudaStream_t st);
+// MD-coupled FEM: every probe through `samples` snapshot specimens (sample s
+// uses snapshot s mod n_snap), exit waves averaged coherently (md.cpp).
+msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps, int samples,
+                  const msf_optics* optics, const msf_raster* raster, const msf_detect* det,
+                  msf_results* res);
 }  // namespace msf

@@ -58,6 +58,7 @@ struct msf_job {
   unsigned dupe_x = 1, dupe_y = 1, dupe_z = 1;
   std::string lammps_pre;
   unsigned lammps_steps = 0, lammps_samples = 0;
+  bool md = false;  // parsed for ms-stem-fem-md (the LAMMPS-coupled driver)
   std::vector<double> mtf, mtf_domain;  // mtf_file: MTF values and domain
   // specimen
   std::vector<double> q;
@@ -354,9 +355,17 @@ void check_flags(msf_job* j) {
     j->messages += "Error: choose either aberration corrected or uncorrected modes\n";
     f.fail = 1;
   }
-  if (f.lammps_preTEM_file) {
-    j->messages += "Error, the LAMMPS-coupled FEM mode needs ms-stem-fem-md and LAMMPS, "
-                   "which are not available in this build\n";
+  if (f.lammps_preTEM_file && !j->md) {
+    j->messages += "Error, the LAMMPS-coupled FEM mode runs in ms-stem-fem-md\n";
+    f.fail = 1;
+  }
+  if (j->md && !(f.lammps_preTEM_file && f.lammps_TEM_steps && f.lammps_TEM_samples)) {
+    j->messages += j->program + " needs --lammps_preTEM_file_name, --lammps_TEM_steps and "
+                   "--lammps_TEM_samples\n";
+    f.fail = 1;
+  }
+  if (j->md && f.lammps_TEM_samples && j->lammps_samples == 0) {
+    j->messages += "Error: lammps_TEM_samples must be at least 1\n";
     f.fail = 1;
   }
 }
@@ -695,6 +704,283 @@ bool write_variance(const std::string& prefix, const double* k_lower, const doub
 
 }  // namespace
 
+// ---------------------------------------------- MD-coupled driver ------
+// ms-stem-fem-md (ftem_lammps.cpp) takes its specimen from LAMMPS: the
+// commands of the pre-TEM file set the system up (read_data, pair_style,
+// pair_coeff ...) and, before every sample of every probe, "run <steps>"
+// advances the MD.  Without LAMMPS the trajectory is a replay of LAMMPS data
+// files: "read_data" in the pre-TEM file gives the initial configuration and
+// the i-th run loads entry (i - 1) mod K of the replay list.
+namespace {
+
+struct MdFrame {
+  std::vector<int> type;     // by atom id - 1
+  std::vector<double> x;     // [id - 1][3], as in the file
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
+// A LAMMPS data file of atom style atomic: the "N atoms" and box lines of
+// the header, then the "Atoms" section of "id type x y z" lines.
+bool read_md_frame(const std::string& path, MdFrame* fr, std::string* err) {
+  std::ifstream in(path.c_str());
+  if (!in.is_open()) {
+    *err = "Error opening LAMMPS data file " + path + "\n";
+    return false;
+  }
+  std::string line;
+  long long n = -1, seen = 0;
+  bool atoms = false;
+  while (std::getline(in, line)) {
+    const size_t hash = line.find('#');
+    std::istringstream ls(hash == std::string::npos ? line : line.substr(0, hash));
+    if (!atoms) {
+      std::vector<std::string> tok;
+      std::string t;
+      while (ls >> t) tok.push_back(t);
+      if (tok.empty()) continue;
+      if (tok.size() >= 2 && tok[1] == "atoms") n = std::atoll(tok[0].c_str());
+      static const char* los[3] = {"xlo", "ylo", "zlo"};
+      for (int d = 0; d < 3; ++d)
+        if (tok.size() >= 4 && tok[2] == los[d]) {
+          fr->lo[d] = std::atof(tok[0].c_str());
+          fr->hi[d] = std::atof(tok[1].c_str());
+        }
+      if (tok[0] == "Atoms") {
+        if (n < 0) break;
+        fr->type.assign(n, 0);
+        fr->x.assign(3 * n, 0.0);
+        atoms = true;
+      }
+      continue;
+    }
+    long long id = 0;
+    int ty = 0;
+    double p[3];
+    if (!(ls >> id >> ty >> p[0] >> p[1] >> p[2])) continue;
+    if (id < 1 || id > n || fr->type[id - 1] != 0) {
+      *err = "Error: atom id " + std::to_string(id) + " out of range or repeated in " + path + "\n";
+      return false;
+    }
+    fr->type[id - 1] = ty;
+    for (int d = 0; d < 3; ++d) fr->x[3 * (id - 1) + d] = p[d];
+    if (++seen == n) break;
+  }
+  if (n < 0 || seen != n) {
+    *err = "Error: " + path + " holds " + std::to_string(seen) + " of " +
+           std::to_string(std::max<long long>(n, 0)) + " atoms\n";
+    return false;
+  }
+  return true;
+}
+
+struct MdSetup {
+  std::vector<std::string> elements;  // pair_coeff element names, by type
+  std::string initial;                // read_data file
+};
+
+// The pre-TEM commands (ftem_lammps.cpp:400-590): the element names of a
+// tersoff / sw / eam pair_coeff line map LAMMPS types to Z; read_data names
+// the initial configuration.
+bool read_pre_tem(const std::string& path, MdSetup* md, std::string* err) {
+  std::ifstream in(path.c_str());
+  if (!in.is_open()) {
+    *err = "Error opening lammps_preTEM_file_name " + path + "\n";
+    return false;
+  }
+  bool style_ok = false;
+  std::string line;
+  while (std::getline(in, line) && in.good()) {
+    if (line.find("pair_style") != std::string::npos &&
+        (line.find("sw") != std::string::npos || line.find("tersoff") != std::string::npos ||
+         line.find("eam") != std::string::npos))
+      style_ok = true;
+    const size_t at = line.find("pair_coeff");
+    if (at != std::string::npos) {
+      if (!style_ok) {
+        *err = "Error in reading lammps_preTEM_file_name : only tersoff, stillinger-weber, "
+               "and eam pair_coeff commands currently allowed\n";
+        return false;
+      }
+      // "pair_coeff * * <file> <element> ...": as the reference reads it,
+      // until the stream is no longer good (a trailing blank repeats the
+      // last name, which changes nothing)
+      std::istringstream pc(line.substr(at));
+      std::string tmp;
+      pc >> tmp >> tmp >> tmp;
+      pc >> tmp;
+      md->elements.clear();
+      while (pc.good()) {
+        pc >> tmp;
+        md->elements.push_back(tmp);
+      }
+    }
+    std::istringstream ls(line);
+    std::string word;
+    if ((ls >> word) && word == "read_data") ls >> md->initial;
+  }
+  if (md->initial.empty()) {
+    *err = "Error: the lammps_preTEM_file_name commands have no read_data\n";
+    return false;
+  }
+  if (md->elements.empty()) {
+    *err = "Error: the lammps_preTEM_file_name commands have no pair_coeff element names\n";
+    return false;
+  }
+  return true;
+}
+
+// One configuration as the reference gathers it from LAMMPS (ftem_lammps.
+// cpp:1640-1740): atoms by id, x and y wrapped into (min, max] of the
+// initial box, Z from the type's element name.
+bool md_positions(const MdFrame& fr, const MdFrame& init, const MdSetup& md,
+                  std::vector<double>* q, std::vector<uint32_t>* z, std::string* err) {
+  const size_t n = fr.type.size();
+  q->assign(3 * n, 0.0);
+  z->assign(n, 0);
+  const double xmin = init.lo[0], xmax = init.hi[0], ymin = init.lo[1], ymax = init.hi[1];
+  const double xperiod = fr.hi[0] - fr.lo[0], yperiod = fr.hi[1] - fr.lo[1];
+  for (size_t a = 0; a < n; ++a) {
+    const int t = fr.type[a];
+    if (t < 1 || (size_t)t > md.elements.size()) {
+      *err = "Error: atom type " + std::to_string(t) + " has no pair_coeff element name\n";
+      return false;
+    }
+    const unsigned zz = element_z(lower(md.elements[t - 1]));
+    if (zz < 1 || zz > 103) {
+      *err = "Error: unknown element " + md.elements[t - 1] + "\n";
+      return false;
+    }
+    (*z)[a] = zz;
+    double x = fr.x[3 * a], y = fr.x[3 * a + 1];
+    while (x <= xmin) x += xperiod;
+    while (x > xmax) x -= xperiod;
+    while (y <= ymin) y += yperiod;
+    while (y > ymax) y -= yperiod;
+    (*q)[3 * a] = x;
+    (*q)[3 * a + 1] = y;
+    (*q)[3 * a + 2] = fr.x[3 * a + 2];
+  }
+  return true;
+}
+
+// Parse argv (tem.cpp:81-403, or ftem_lammps.cpp:95-1420 when `md`): the
+// options, --parameter_file, the specimen file, the flag checks and the
+// defaults.  The MD driver also reads the pre-TEM commands and the initial
+// configuration, whose box sets the cell (ftem_lammps.cpp:1122-1148), and
+// writes its outputs under the plain output prefix.
+msf_status parse_job(int32_t argc, const char* const* argv, bool md, msf_job** out,
+                     MdSetup* setup, MdFrame* init) {
+  if (!out || argc < 1 || !argv) return MSF_ERR_ARG;
+  msf_job* j = new msf_job;
+  std::vector<std::string> args(argv, argv + argc);
+  j->program = args[0];
+  j->md = md;
+  parse_args(args, j);
+  // tem.cpp:240-330: the specimen is read before the flag checks
+  msf_status st = MSF_OK;
+  const bool xyz = j->model_file.substr(j->model_file.find_last_of('.') + 1) == "xyz";
+  if ((xyz ? read_xyz(j->model_file, j) : read_lammps(j->model_file, j)) != MSF_OK) {
+    j->messages += "Error, file could not be read : " + j->model_file + "\n";
+    j->flags.fail = 1;
+    st = MSF_ERR_IO;
+  }
+  check_flags(j);
+  if (!j->flags.fail && md) {
+    std::string err;
+    if (!read_pre_tem(j->lammps_pre, setup, &err) ||
+        !read_md_frame(setup->initial, init, &err)) {
+      j->messages += err;
+      j->flags.fail = 1;
+      st = MSF_ERR_IO;
+    } else {
+      j->xmin = init->lo[0];
+      j->ymin = init->lo[1];
+      j->zmin = init->lo[2];
+      j->xperiod = init->hi[0] - init->lo[0];
+      j->yperiod = init->hi[1] - init->lo[1];
+      j->zperiod = init->hi[2] - init->lo[2];
+    }
+  }
+  if (j->flags.fail) {
+    msf::set_error(j->messages + "Exiting ms-stem-fem due to failure.\n");
+    delete j;
+    return st != MSF_OK ? st : MSF_ERR_PARSE;
+  }
+  st = finish_job(j);
+  if (st != MSF_OK) {
+    msf::set_error(j->messages);
+    delete j;
+    return st;
+  }
+  if (md) j->full_prefix = j->output_prefix;
+  *out = j;
+  return MSF_OK;
+}
+
+// Host result buffers for a drop-in run: every V(k) mode, the ADF image,
+// correlograph tables, and the diffraction planes --images writes.
+struct RunBuffers {
+  std::vector<double> img, kl, v[6], phi, corr, corr_sqr, corr_probes, final_psi, first_psi,
+      mean_a, mean_i;
+  msf_results r{};
+  void setup(const msf_job* j, const msf_grid& grid, const msf_raster& raster,
+             const msf_detect& det, bool want_first) {
+    const size_t nr = raster.n_x * (size_t)raster.n_y;
+    const size_t plane = (size_t)grid.nx * grid.ny;
+    img.assign(nr, 0.0);
+    kl.assign(8192, 0.0);
+    for (auto& a : v) a.assign(8192, 0.0);
+    r = msf_results{};
+    r.adf_image = img.data();
+    r.cap_k = 8192;
+    r.k_lower = kl.data();
+    r.v_omega = v[0].data();
+    r.vbar_r = v[1].data();
+    r.v_re = v[2].data();
+    r.omega_vimage = v[3].data();
+    r.v_gt17 = v[4].data();
+    r.v_rbar = v[5].data();
+    // correlograph: bins from the segment counts with and without the cells
+    if (det.outputs & MSF_OUT_CORRELOGRAPH) {
+      msf_detect rings = det;
+      rings.outputs &= ~(uint32_t)(MSF_OUT_CORRELOGRAPH | MSF_OUT_CORRELOGRAPH_VAR);
+      rings.outputs |= MSF_OUT_V_OMEGA;
+      const int32_t n_k = msf_segment_count(&grid, &rings) - 1;
+      const int32_t cells = msf_segment_count(&grid, &det) - 1 - n_k;
+      const int32_t n_phi = n_k > 0 ? cells / n_k : 0;
+      const size_t nc = std::max<size_t>(1, (size_t)n_k * n_phi);
+      phi.assign(n_phi + 1, 0.0);
+      corr.assign(nc, 0.0);
+      corr_sqr.assign(nc, 0.0);
+      r.cap_phi = n_phi;
+      r.phi_lower = phi.data();
+      r.correlograph = corr.data();
+      r.correlograph_sqr = corr_sqr.data();
+      if (j->flags.correlograph_everyimage || j->flags.correlograph_everytxt) {
+        corr_probes.assign(nc * nr, 0.0);
+        r.correlograph_probes = corr_probes.data();
+      }
+    }
+    if (j->flags.image_output) {  // the first and last exit waves' diffraction
+      final_psi.assign(2 * plane, 0.0);
+      r.final_psi = final_psi.data();
+      if (want_first) {
+        first_psi.assign(2 * plane, 0.0);
+        r.first_psi = first_psi.data();
+      }
+    }
+    if (j->flags.image_output &&  // the FEM pixel modes' diffraction averages
+        (det.outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE | MSF_OUT_V_GT17 | MSF_OUT_V_RBAR))) {
+      mean_a.assign(plane, 0.0);
+      mean_i.assign(plane, 0.0);
+      r.mean_amplitude = mean_a.data();
+      r.mean_intensity = mean_i.data();
+    }
+  }
+};
+
+}  // namespace
+
 // ------------------------------------------------------------- C ABI ------
 extern "C" {
 
@@ -717,33 +1003,7 @@ msf_status msf_read_specimen(const char* path, msf_job** out) {
 }
 
 msf_status msf_parse_cmdline(int32_t argc, const char* const* argv, msf_job** out) {
-  if (!out || argc < 1 || !argv) return MSF_ERR_ARG;
-  msf_job* j = new msf_job;
-  std::vector<std::string> args(argv, argv + argc);
-  j->program = args[0];
-  parse_args(args, j);
-  // tem.cpp:240-330: the specimen is read before the flag checks
-  msf_status st = MSF_OK;
-  const bool xyz = j->model_file.substr(j->model_file.find_last_of('.') + 1) == "xyz";
-  if ((xyz ? read_xyz(j->model_file, j) : read_lammps(j->model_file, j)) != MSF_OK) {
-    j->messages += "Error, file could not be read : " + j->model_file + "\n";
-    j->flags.fail = 1;
-    st = MSF_ERR_IO;
-  }
-  check_flags(j);
-  if (j->flags.fail) {
-    msf::set_error(j->messages + "Exiting ms-stem-fem due to failure.\n");
-    delete j;
-    return st != MSF_OK ? st : MSF_ERR_PARSE;
-  }
-  st = finish_job(j);
-  if (st != MSF_OK) {
-    msf::set_error(j->messages);
-    delete j;
-    return st;
-  }
-  *out = j;
-  return MSF_OK;
+  return parse_job(argc, argv, false, out, nullptr, nullptr);
 }
 
 msf_status msf_job_destroy(msf_job* job) {
@@ -928,6 +1188,40 @@ msf_status msf_write_outputs(const msf_job* j, const msf_results* r) {
       for (double scale : {1.0e-5, 1.0e-1, 1.0e0, 1.0e10, 1.0e+20})
         if (!diffraction(r->first_psi, scale, "_first")) return MSF_ERR_IO;
     if (r->final_psi && !diffraction(r->final_psi, 1.0e+0, "_final")) return MSF_ERR_IO;
+    // FEM pixel modes (adfstem.cpp:3062-3097, 3468-3530): the raster means
+    // of |psi(k)| and |psi(k)|^2 through the real-array output_diffraction
+    // (write_tif.cpp:1413-1551, log(1 + s x^2)), and with --Omega_vimage the
+    // 2-D variance <I>/<|psi|>^2 - 1 with the aperture disc zeroed.
+    const bool pix = f.fem && (f.gt17 || f.d3 || f.d4 || f.rva);
+    if (pix && r->mean_amplitude) {
+      std::vector<double> c(2 * nx * ny, 0.0);
+      auto real_diffraction = [&](const double* x, double scale, const std::string& tag) {
+        for (size_t k = 0; k < nx * ny; ++k) c[2 * k] = x[k];
+        return diffraction(c.data(), scale, tag);
+      };
+      if (!real_diffraction(r->mean_amplitude, 1.0e13, "_diffracted_wave_avg"))
+        return MSF_ERR_IO;
+      if ((f.gt17 || f.d3 || f.d4) && r->mean_intensity &&
+          !real_diffraction(r->mean_intensity, 1.0e13, "_diffracted_wave_sqr_avg"))
+        return MSF_ERR_IO;
+      if (f.d4 && r->mean_intensity) {
+        const msf::Grid g = msf::make_grid(
+            j->nx, j->ny, j->VV, j->xperiod * j->dupe_x, j->yperiod * j->dupe_y,
+            j->zperiod * j->dupe_z, j->xmin, j->ymin, j->zmin, j->xperiod, j->yperiod, j->zperiod);
+        const double lambda_sqr = g.lambda * g.lambda, alpha_max_sqr = j->alpha_max * j->alpha_max;
+        std::vector<double> var(nx * ny);
+        for (size_t k = 0; k < nx * ny; ++k)
+          var[k] = (r->mean_intensity[k] / (r->mean_amplitude[k] * r->mean_amplitude[k])) - 1.0;
+        for (size_t i = 0; i < nx; ++i)
+          for (size_t k = 0; k < ny; ++k) {
+            const double ksqr = std::pow(g.kx[i], 2) + std::pow(g.ky[k], 2);
+            if (lambda_sqr * ksqr <= alpha_max_sqr) var[k + ny * i] = 0.0;
+          }
+        if (!real_diffraction(var.data(), 1.0e0, "_variance_2-D") ||
+            !real_diffraction(var.data(), 1.0e-10, "_variance_2-D"))
+          return MSF_ERR_IO;
+      }
+    }
   }
   if (f.image_output && r->adf_image) {
     const size_t nx = j->x_p.size(), ny = j->y_p.size();
@@ -969,54 +1263,112 @@ int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) 
   int rc = 1;
   if ((st = msf_context_create(&o, &ctx)) == MSF_OK &&
       (st = msf_specimen_create(ctx, &grid, &atoms, &spec)) == MSF_OK) {
-    const size_t nr = raster.n_x * (size_t)raster.n_y;
-    std::vector<double> img(nr), kl(8192), v[6];
-    for (auto& a : v) a.assign(8192, 0.0);
-    msf_results r{};
-    r.adf_image = img.data();
-    r.cap_k = 8192;
-    r.k_lower = kl.data();
-    r.v_omega = v[0].data();
-    r.vbar_r = v[1].data();
-    r.v_re = v[2].data();
-    r.omega_vimage = v[3].data();
-    r.v_gt17 = v[4].data();
-    r.v_rbar = v[5].data();
-    // correlograph: bins from the segment counts with and without the cells
-    std::vector<double> phi, corr, corr_sqr, corr_probes;
-    if (det.outputs & MSF_OUT_CORRELOGRAPH) {
-      msf_detect plain = det;
-      plain.outputs &= ~(uint32_t)(MSF_OUT_CORRELOGRAPH | MSF_OUT_CORRELOGRAPH_VAR);
-      plain.outputs |= MSF_OUT_V_OMEGA;
-      const int32_t n_k = msf_segment_count(&grid, &plain) - 1;
-      const int32_t cells = msf_segment_count(&grid, &det) - 1 - n_k;
-      const int32_t n_phi = n_k > 0 ? cells / n_k : 0;
-      const size_t nc = std::max<size_t>(1, (size_t)n_k * n_phi);
-      phi.assign(n_phi + 1, 0.0);
-      corr.assign(nc, 0.0);
-      corr_sqr.assign(nc, 0.0);
-      r.cap_phi = n_phi;
-      r.phi_lower = phi.data();
-      r.correlograph = corr.data();
-      r.correlograph_sqr = corr_sqr.data();
-      if (j->flags.correlograph_everyimage || j->flags.correlograph_everytxt) {
-        corr_probes.assign(nc * nr, 0.0);
-        r.correlograph_probes = corr_probes.data();
-      }
-    }
-    std::vector<double> final_psi, first_psi;
-    if (j->flags.image_output) {  // the first and last exit waves' diffraction
-      final_psi.assign(2 * (size_t)grid.nx * grid.ny, 0.0);
-      first_psi.assign(2 * (size_t)grid.nx * grid.ny, 0.0);
-      r.final_psi = final_psi.data();
-      r.first_psi = first_psi.data();
-    }
-    if ((st = msf_run(ctx, spec, &optics, &raster, &det, &r)) == MSF_OK &&
-        (st = msf_write_outputs(j, &r)) == MSF_OK)
+    RunBuffers b;
+    b.setup(j, grid, raster, det, true);
+    if ((st = msf_run(ctx, spec, &optics, &raster, &det, &b.r)) == MSF_OK &&
+        (st = msf_write_outputs(j, &b.r)) == MSF_OK)
       rc = 0;
   }
   if (rc != 0) std::cerr << "ms-stem-fem: " << msf::last_error() << std::endl;
   msf_specimen_destroy(spec);
+  msf_context_destroy(ctx);
+  msf_job_destroy(j);
+  return rc;
+}
+
+int32_t msf_md_main(int32_t argc, const char* const* argv, const msf_options* opt) {
+  std::vector<const char*> args;
+  std::string replay_list;
+  for (int32_t i = 0; i < argc; ++i) {
+    if (i > 0 && std::string(argv[i]) == "--md_replay" && i + 1 < argc)
+      replay_list = argv[++i];
+    else
+      args.push_back(argv[i]);
+  }
+  msf_job* j = nullptr;
+  MdSetup md;
+  MdFrame init;
+  std::string err;
+  msf_status st = parse_job((int32_t)args.size(), args.data(), true, &j, &md, &init);
+  if (st != MSF_OK) {
+    std::cout << msf::last_error();
+    return 1;
+  }
+  // the configurations the samples see: the initial one when LAMMPS runs
+  // no steps, else the replay list, sample s taking entry s mod K (every
+  // probe's run count p * samples + s then maps to the same entry)
+  std::vector<MdFrame> frames;
+  bool ok = true;
+  if (j->lammps_steps == 0) {
+    frames.push_back(init);
+  } else {
+    std::vector<std::string> files;
+    std::ifstream in(replay_list.c_str());
+    std::string line;
+    while (std::getline(in, line)) {
+      std::istringstream ls(line);
+      std::string path;
+      if (ls >> path) files.push_back(path);
+    }
+    if (files.empty()) {
+      err = "LAMMPS is not available here; give --md_replay <file> listing the "
+            "LAMMPS data files its runs would produce, one per line\n";
+      ok = false;
+    } else if (j->lammps_samples % files.size() != 0) {
+      err = "Error: lammps_TEM_samples (" + std::to_string(j->lammps_samples) +
+            ") must be a multiple of the " + std::to_string(files.size()) + " replayed "
+            "configurations\n";
+      ok = false;
+    }
+    for (size_t k = 0; ok && k < files.size(); ++k) {
+      frames.emplace_back();
+      ok = read_md_frame(files[k], &frames.back(), &err);
+    }
+  }
+  // every configuration's atoms, checked before any device work
+  std::vector<std::vector<double>> qs(frames.size());
+  std::vector<std::vector<uint32_t>> zs(frames.size());
+  for (size_t k = 0; ok && k < frames.size(); ++k) {
+    const MdFrame& fr = frames[k];
+    if (fr.hi[0] - fr.lo[0] != j->xperiod || fr.hi[1] - fr.lo[1] != j->yperiod) {
+      err = "Error: replayed configuration " + std::to_string(k) + " changes the x or y "
+            "period of the box, which this driver does not support\n";
+      ok = false;
+    } else {
+      ok = md_positions(fr, init, md, &qs[k], &zs[k], &err);
+    }
+  }
+  msf_options o{};
+  o.precision = MSF_FP64;
+  o.use_graphs = 1;
+  if (opt) o = *opt;
+  msf_context* ctx = nullptr;
+  std::vector<msf_specimen*> specs(frames.size(), nullptr);
+  msf_grid grid;
+  msf_optics optics;
+  msf_raster raster;
+  msf_detect det;
+  msf_job_describe(j, &grid, nullptr, &optics, &raster, &det);
+  int rc = 1;
+  if (ok && (st = msf_context_create(&o, &ctx)) == MSF_OK) {
+    for (size_t k = 0; ok && k < frames.size(); ++k) {
+      msf_grid gk = grid;
+      gk.zperiod = frames[k].hi[2] - frames[k].lo[2];  // follows the box (ftem_lammps.cpp:1611)
+      msf_atoms a{(int64_t)zs[k].size(), qs[k].data(), zs[k].data()};
+      if ((st = msf_specimen_create(ctx, &gk, &a, &specs[k])) != MSF_OK) ok = false;
+    }
+    if (ok) {
+      RunBuffers b;
+      b.setup(j, grid, raster, det, false);
+      if ((st = msf_run_md(ctx, (int32_t)specs.size(), specs.data(),
+                           (int32_t)j->lammps_samples, &optics, &raster, &det, &b.r)) == MSF_OK &&
+          (st = msf_write_outputs(j, &b.r)) == MSF_OK)
+        rc = 0;
+    }
+  }
+  if (rc != 0) std::cerr << j->program << ": " << (err.empty() ? msf::last_error() : err.c_str())
+                         << std::endl;
+  for (msf_specimen* sp : specs) msf_specimen_destroy(sp);
   msf_context_destroy(ctx);
   msf_job_destroy(j);
   return rc;

@@ -754,6 +754,34 @@ __global__ void to_f32_minus_one_kernel(const double2* __restrict__ in, float2* 
   if (k < n) out[k] = make_float2((float)(in[k].x - 1.0), (float)in[k].y);
 }
 
+// ---- MD-coupled FEM (ftem_lammps.cpp:3601-3610): the coherent average of
+// each probe's exit wave over the specimen samples.  acc_b[p] += psi_b[p] /
+// samples for nb planes, psi the exit wave in k-space including the vacuum
+// part of split-wave runs; FP64.
+template <typename Real>
+__global__ void wave_accumulate_kernel(const Cx<Real>* __restrict__ psi, int64_t stride, int nb,
+                                       int64_t plane, const SplitK sk, double divisor,
+                                       double2* __restrict__ acc) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= plane * nb) return;
+  const int b = (int)(k / plane);
+  const int p = (int)(k - (int64_t)b * plane);
+  const int sx = sk.psi0k ? sk.shifts[2 * b] : 0, sy = sk.psi0k ? sk.shifts[2 * b + 1] : 0;
+  const double2 v = exit_value<Real>(psi + (int64_t)b * stride, p, sk, sx, sy);
+  double2 a = acc[k];
+  a.x += v.x / divisor;
+  a.y += v.y / divisor;
+  acc[k] = a;
+}
+
+// dst[i * dst_stride] += src[i * src_stride] / divisor, i < n
+__global__ void strided_accumulate_kernel(double* __restrict__ dst, int64_t dst_stride,
+                                          const double* __restrict__ src, int64_t src_stride,
+                                          int n, double divisor) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[(int64_t)i * dst_stride] += src[(int64_t)i * src_stride] / divisor;
+}
+
 __global__ void assemble_split_kernel(const float2* __restrict__ delta, SplitK sk,
                                       int32_t sx, int32_t sy, double2* out) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1047,6 +1075,29 @@ cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t stride, int n
 cudaError_t launch_to_f32_minus_one(const double* in, float* out, int64_t n, cudaStream_t s) {
   to_f32_minus_one_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
       reinterpret_cast<const double2*>(in), reinterpret_cast<float2*>(out), n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wave_accumulate(bool fp64, const void* psi, int64_t stride, int nb,
+                                   int64_t plane, const SplitK& sk, double divisor, double* acc,
+                                   cudaStream_t s) {
+  const int64_t n = plane * nb;
+  if (fp64)
+    wave_accumulate_kernel<double><<<blocks_for(n, 256), 256, 0, s>>>(
+        static_cast<const double2*>(psi), stride, nb, plane, sk, divisor,
+        reinterpret_cast<double2*>(acc));
+  else
+    wave_accumulate_kernel<float><<<blocks_for(n, 256), 256, 0, s>>>(
+        static_cast<const float2*>(psi), stride, nb, plane, sk, divisor,
+        reinterpret_cast<double2*>(acc));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_strided_accumulate(double* dst, int64_t dst_stride, const double* src,
+                                      int64_t src_stride, int n, double divisor, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  strided_accumulate_kernel<<<blocks_for(n, 128), 128, 0, s>>>(dst, dst_stride, src, src_stride,
+                                                                 n, divisor);
   return cudaGetLastError();
 }
 

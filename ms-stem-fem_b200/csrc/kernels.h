@@ -219,6 +219,15 @@ cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
 // parts of n complex doubles: tau = t - 1 for split-wave passes.
 cudaError_t launch_to_f32_minus_one(const double* in, float* out, int64_t n_complex,
                                     cudaStream_t s);
+// MD-coupled FEM: acc_b += psi_b / divisor for nb planes [b][plane] (FP64
+// acc), psi the exit wave in k-space incl. the vacuum part of split-wave
+// runs (sk), batch stride `stride` elements.
+cudaError_t launch_wave_accumulate(bool fp64, const void* psi, int64_t stride, int nb,
+                                   int64_t plane, const SplitK& sk, double divisor, double* acc,
+                                   cudaStream_t s);
+// dst[i * dst_stride] += src[i * src_stride] / divisor, i < n.
+cudaError_t launch_strided_accumulate(double* dst, int64_t dst_stride, const double* src,
+                                      int64_t src_stride, int n, double divisor, cudaStream_t s);
 // psi (complex) = delta (FP32, k-space) + shifted vacuum part (FP64), for
 // one probe: used to return the exit wave of a split-wave run.
 cudaError_t launch_assemble_split(const float* delta, const double* psi0k, int nx, int ny,

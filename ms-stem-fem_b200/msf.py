@@ -44,7 +44,7 @@ EXPORTED = [
     "msf_time_passes", "msf_context_transfer_bytes", "msf_probe_noalloc",
     "msf_run_batch", "msf_server_create", "msf_server_submit", "msf_server_poll",
     "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
-    "msf_finish", "msf_run_plain", "msf_amorphous_positions",
+    "msf_finish", "msf_run_plain", "msf_amorphous_positions", "msf_run_md", "msf_md_main",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -164,6 +164,10 @@ def lib() -> C.CDLL:
         L.msf_read_specimen.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
         L.msf_write_outputs.argtypes = [C.c_void_p, C.POINTER(Results)]
         L.msf_main.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(Options)]
+        L.msf_md_main.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(Options)]
+        L.msf_run_md.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.c_int32,
+                                 C.POINTER(Optics), C.POINTER(Raster), C.POINTER(Detect),
+                                 C.POINTER(Results)]
         L.msf_run_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p),
                                     C.POINTER(Optics), C.POINTER(Raster), C.POINTER(Detect),
                                     C.POINTER(Results), C.c_int32]
@@ -324,6 +328,25 @@ class Context:
             out.add_correlograph(spec.grid, detect, n_r, want_correlograph_probes)
         _check(lib().msf_run(self._h, spec._h, C.byref(optics), C.byref(raster),
                              C.byref(detect), C.byref(out._struct)))
+        out.finish(raster, detect)
+        return out
+
+    def run_md(self, snapshots, samples: int, optics: Optics, raster: Raster, detect: Detect,
+               want_final_psi=False, want_means=False, want_rings=False,
+               cap_k=8192) -> "RunResult":
+        """MD-coupled FEM (msf_run_md): each probe through `samples`
+        configurations, sample s through snapshots[s % len(snapshots)], exit
+        waves averaged coherently before the FEM statistics."""
+        g = snapshots[0].grid
+        n_r = raster.n_x * raster.n_y
+        if want_rings:
+            cap_k = min(cap_k, 1024)
+        out = RunResult(n_r, cap_k, g.nx, g.ny, want_final_psi, want_means, want_rings)
+        if detect.outputs & OUT_CORRELOGRAPH:
+            out.add_correlograph(g, detect, n_r, False)
+        hs = (C.c_void_p * len(snapshots))(*[sp._h.value for sp in snapshots])
+        _check(lib().msf_run_md(self._h, len(snapshots), hs, int(samples), C.byref(optics),
+                                C.byref(raster), C.byref(detect), C.byref(out._struct)))
         out.finish(raster, detect)
         return out
 
@@ -604,9 +627,10 @@ def run_job(argv, precision="fp64", device=0, batch=0, graphs=True, write=False,
     return job, spec, res, ctx
 
 
-def main(argv, precision="fp64", device=0, batch=0) -> int:
-    """The whole drop-in program (msf_main); returns the exit status."""
+def main(argv, precision="fp64", device=0, batch=0, md=False) -> int:
+    """The whole drop-in program (msf_main, or msf_md_main for the
+    MD-coupled driver); returns the exit status."""
     argv = [str(a) for a in argv]
     arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
     opt = Options(device, MSF_FP32 if precision == "fp32" else MSF_FP64, batch, 1, 0)
-    return lib().msf_main(len(argv), arr, C.byref(opt))
+    return (lib().msf_md_main if md else lib().msf_main)(len(argv), arr, C.byref(opt))

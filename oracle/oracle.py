@@ -1,5 +1,7 @@
-"""ctypes binding of the CPU oracle (oracle/msf_oracle.c) and a runner for the
-reference's own binary (oracle/_ref/ms-stem-fem-ref).
+"""ctypes binding of the CPU oracle (oracle/msf_oracle.c) and runners for the
+reference's own binaries (oracle/_ref/ms-stem-fem-ref and, for the
+MD-coupled driver with LAMMPS replaced by a data-file replay,
+oracle/_ref/ms-stem-fem-md-ref).
 
 TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
 CPU-baseline leg use this module as the checker; the product never does.
@@ -18,6 +20,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 REF_BIN = HERE / "_ref" / "ms-stem-fem-ref"
+REF_MD_BIN = HERE / "_ref" / "ms-stem-fem-md-ref"
 
 OR_ADF, OR_D1, OR_D2, OR_D3, OR_D4, OR_GT17, OR_RVA = 1, 2, 4, 8, 16, 32, 64
 MODE_BITS = {"V_omega": OR_D1, "Vbar_r": OR_D2, "V_re": OR_D3,
@@ -204,13 +207,15 @@ def ref_available() -> bool:
     return REF_BIN.exists()
 
 
-def run_reference(args, cwd, env_extra=None, timeout=None) -> dict:
-    """Run oracle/_ref/ms-stem-fem-ref with argv ``args`` in ``cwd``; returns
-    stdout, stderr and the adfstem wall time the link-time hook printed."""
+def run_reference(args, cwd, env_extra=None, timeout=None, md=False) -> dict:
+    """Run oracle/_ref/ms-stem-fem-ref (md: ms-stem-fem-md-ref, whose LAMMPS
+    "run" loads the next file of the list MSF_MD_REPLAY names) with argv
+    ``args`` in ``cwd``; returns stdout, stderr and the adfstem wall time
+    the link-time hook printed."""
     env = dict(os.environ)
     if env_extra:
         env.update(env_extra)
-    p = subprocess.run([str(REF_BIN)] + list(args), cwd=str(cwd), env=env,
+    p = subprocess.run([str(REF_MD_BIN if md else REF_BIN)] + list(args), cwd=str(cwd), env=env,
                        capture_output=True, text=True, timeout=timeout)
     m = re.search(r"adfstem_seconds=([0-9.eE+-]+) probes=(\d+) slices=(\d+)", p.stderr)
     return {"returncode": p.returncode, "stdout": p.stdout, "stderr": p.stderr,

@@ -20,8 +20,10 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libmsf.so")
 
 
-def golden_cases():
-    return sorted(p.stem for p in GOLDEN.glob("*.json"))
+def golden_cases(md=False):
+    """Golden cases of the ms-stem-fem driver, or (md) of ms-stem-fem-md."""
+    return sorted(p.stem for p in GOLDEN.glob("*.json")
+                  if bool(json.loads(p.read_text()).get("md")) == md)
 
 
 def load_case(name):
@@ -40,6 +42,10 @@ def case_dir(name, tmp_root: Path) -> Path:
     meta, _ = load_case(name)
     d = tmp_root / name
     d.mkdir(parents=True, exist_ok=True)
+    if meta.get("md"):  # initial and replayed configurations, pre-TEM commands
+        for f in (GOLDEN / name).iterdir():
+            shutil.copy(f, d / f.name)
+        return d
     target = d / meta["argv"][1]
     if meta["committed_specimen"]:
         shutil.copy(GOLDEN / meta["argv"][1], target)

@@ -169,8 +169,11 @@ def run_case(name):
     for f in sorted(work.glob(name + "_adfstem_*corr_[0-9]*_[0-9]*.txt")):
         px, py = f.stem.split("_")[-2:]
         out["correlograph_probe_%s_%s" % (px, py)] = np.loadtxt(f, ndmin=2)
-    for tag in ("first", "final"):  # diffraction patterns written with --images
-        for f in work.glob("*_%s_diffraction_scalefactor_*.tif" % tag):
+    # diffraction patterns written with --images: first and last probe, and
+    # with FEM pixel modes the raster averages and the 2-D variance
+    for tag in ("first", "final", "diffracted_wave_avg", "diffracted_wave_sqr_avg",
+                "variance_2-D"):
+        for f in work.glob("*_adfstem_*corr_%s_diffraction_scalefactor_*.tif" % tag):
             out["%s_diffraction_%s" % (tag, f.stem.split("_scalefactor_")[1])] = read_tif16(f)
     sl = np.loadtxt(work / "slices.txt", ndmin=2)
     out["slice_lower"], out["slice_thickness"], out["slice_count"] = sl[:, 0], sl[:, 1], sl[:, 2]
@@ -189,10 +192,97 @@ def run_case(name):
     print(name, "ok", r["adfstem_seconds"], "s", sorted(out))
 
 
+# MD-coupled cases (the reference's ms-stem-fem-md with LAMMPS replaced by
+# the data-file replay of oracle/shims/lammps): an initial configuration in a
+# box with a non-zero origin, `snapshots` jittered copies of it (positions
+# left unwrapped, so the driver's periodic wrap is exercised) and the argv.
+# name -> (recipe, box origin, snapshots, jitter [A], seed, argv, steps, samples)
+MD_CASES = {
+    # three configurations, each seen twice per probe; every FEM mode
+    "md": (dict(n=780, box=(25, 25, 25), seed=1), (-12.5, -5.0, -3.0), 3, 0.15, 41,
+           "-m 128 128 200000 --adfstemuncorrfem " + " ".join(FEM_ALL) +
+           " --cs3 1.3e7 --scherzer_defocus --alphamax 0.010 --rasterspacing 6.25 "
+           "--minslice 2.0 --images", 10, 6),
+    # no MD steps: every sample sees the initial configuration
+    "md_static": (dict(n=390, box=(25, 25, 12.5), seed=11), (0.0, 0.0, 0.0), 0, 0.0, 0,
+                  "-m 128 64 200000 --adfstemuncorrfem --V_omega --Vbar_r --cs3 1.3e7 "
+                  "--defocus 300 --alphamax 0.012 --rasterspacing 5 --minslice 2.0 --images",
+                  0, 2),
+}
+
+PRE_TEM = ("units metal\natom_style atomic\nboundary p p p\nread_data {initial}\n"
+           "pair_style sw\npair_coeff * * Si.sw Si\nvelocity all create 300.0 4928459\n"
+           "fix 1 all nve\ntimestep 0.001\n")
+
+
+def write_frame(path, header, pos):
+    rows = ["%d 1 %.6f %.6f %.6f" % (k + 1, p[0], p[1], p[2]) for k, p in enumerate(pos)]
+    Path(path).write_text("\n".join(header + rows) + "\n")
+
+
+def run_md_case(name):
+    recipe, origin, n_snap, jitter, seed, args, steps, samples = MD_CASES[name]
+    work = Path(tempfile.mkdtemp(prefix="golden_" + name))
+    base = work / "base.data"
+    pos = specimen.make_specimen(base, recipe["n"], recipe["box"], seed=recipe["seed"])
+    pos = np.asarray(pos, float) + np.asarray(origin)
+    lo, hi = np.asarray(origin), np.asarray(origin) + np.asarray(recipe["box"], float)
+    header = ["# " + name, "", "%d atoms" % len(pos), "1 atom types", ""]
+    header += ["%.6f %.6f %s %s" % (lo[d], hi[d], a, b)
+               for d, (a, b) in enumerate((("xlo", "xhi"), ("ylo", "yhi"), ("zlo", "zhi")))]
+    header += ["", "Masses", "", "1 28.0855", "", "Atoms", ""]
+    files = {}
+    initial = name + "_0.data"
+    write_frame(work / initial, header, pos)
+    files[initial] = (work / initial).read_text()
+    rng = np.random.default_rng(seed)
+    replay = []
+    for k in range(1, n_snap + 1):
+        f = "%s_%d.data" % (name, k)
+        write_frame(work / f, header, pos + rng.normal(0.0, jitter, pos.shape))
+        files[f] = (work / f).read_text()
+        replay.append(f)
+    files[name + ".in"] = PRE_TEM.format(initial=initial)
+    if replay:
+        files[name + "_replay.txt"] = "\n".join(replay) + "\n"
+    for f, text in files.items():
+        (work / f).write_text(text)
+    argv = (["-a", initial, "--output_prefix", name] + args.split() +
+            ["--lammps_preTEM_file_name", name + ".in", "--lammps_TEM_steps", str(steps),
+             "--lammps_TEM_samples", str(samples)])
+    env = {"MSF_MD_REPLAY": str(work / (name + "_replay.txt"))} if replay else {}
+    r = oracle.run_reference(argv, cwd=work, env_extra=env, md=True)
+    if r["returncode"] != 0:
+        raise RuntimeError("reference failed for %s:\n%s\n%s" % (name, r["stdout"], r["stderr"]))
+    out = {}
+    out["adf_image"] = np.fromfile(work / (name + "_stem_image_output.f64"))
+    for f in sorted(work.glob(name + "_fem_*.txt")):
+        out[f.stem.split("_fem_")[1]] = oracle.read_variance_txt(f)
+    for tag in ("final", "diffracted_wave_avg", "diffracted_wave_sqr_avg", "variance_2-D"):
+        for f in work.glob("%s_%s_diffraction_scalefactor_*.tif" % (name, tag)):
+            out["%s_diffraction_%s" % (tag, f.stem.split("_scalefactor_")[1])] = read_tif16(f)
+    np.savez_compressed(HERE / (name + ".npz"), **out)
+    extra = ["--md_replay", name + "_replay.txt"] if replay else []
+    meta = dict(case=name, argv=argv, md_argv_extra=extra, recipe=recipe, origin=origin,
+                snapshots=n_snap, jitter=jitter, seed=seed, prefix=name,
+                committed_specimen=False, specimen_sha256=None,
+                files={f: "" for f in files}, md=True)
+    (HERE / (name + ".json")).write_text(json.dumps(meta, indent=1) + "\n")
+    mddir = HERE / name
+    mddir.mkdir(exist_ok=True)
+    for f, text in files.items():
+        (mddir / f).write_text(text)
+    shutil.rmtree(work)
+    print(name, "ok", sorted(out))
+
+
 def main():
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + list(MD_CASES)
     for n in names:
-        run_case(n)
+        if n in MD_CASES:
+            run_md_case(n)
+        else:
+            run_case(n)
 
 
 if __name__ == "__main__":
