@@ -217,6 +217,29 @@ msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
 msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
                              double* probe_device, void* stream);
 
+/* ---- launch tiling autotuner (the analogue of the reference's FFTW
+ * wisdom, tem.cpp:583-616 and 1748-1765) ---------------------------------- */
+typedef struct {
+  int32_t nx, ny;             /* grid                                          */
+  int32_t batch;              /* probes per launch chosen                      */
+  int32_t pipe;               /* pipelined FP32 passes: bit 0 column, bit 1 row */
+  double ns_per_probe_slice;  /* measured time of the two slice passes        */
+} msf_tuning;
+/* Times the two slice passes of `spec`'s grid (CUDA events, after a
+ * warm-up) for each candidate probes-per-launch (8 .. 256, within half the
+ * free memory) and, for FP32 grids the pipelined passes support, with and
+ * without the pipelined column pass; records the fastest per probe*slice
+ * in the context, where msf_run / msf_run_md / msf_run_partial use it for
+ * that grid unless the context's batch or MSF_PIPE fixes the choice. */
+msf_status msf_tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out);
+/* The context's tuning as text, one line per grid ("msf-wisdom 1 <device
+ * name> <fp32|fp64> <nx> <ny> <batch> <pipe> <ns>"): returns the length
+ * (without the terminating NUL) and copies what fits into buf[cap]. */
+int64_t msf_wisdom_export(const msf_context* ctx, char* buf, int64_t cap);
+/* Adds the lines of `text` that were measured on this device model and
+ * precision to the context's tuning; *n_imported (may be NULL) counts them. */
+msf_status msf_wisdom_import(msf_context* ctx, const char* text, int32_t* n_imported);
+
 /* ---- MD-coupled FEM (the reference's ms-stem-fem-md) -------------------- */
 /* Replaces the raster loop of ftem_lammps.cpp main (1513-3610, 4077-4990):
  * every probe position is propagated through `samples` configurations of

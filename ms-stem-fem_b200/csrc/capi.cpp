@@ -77,7 +77,10 @@ msf_status msf_context_create(const msf_options* opt, msf_context** out) {
   c->fp64 = o.precision == MSF_FP64;
   c->batch = o.batch;
   c->graphs = o.use_graphs != 0;
-  if (const char* p = std::getenv("MSF_PIPE")) c->pipe = std::atoi(p);
+  if (const char* p = std::getenv("MSF_PIPE")) {
+    c->pipe = std::atoi(p);
+    c->pipe_env = true;
+  }
   if (const char* p = std::getenv("MSF_POTENTIAL"))
     c->potential = std::string(p) == "direct" ? 1 : std::string(p) == "fft" ? 2 : 0;
   c->budget = o.hbm_budget;
@@ -193,6 +196,14 @@ msf_status msf_run(msf_context* ctx, const msf_specimen* spec, const msf_optics*
     return MSF_ERR_ARG;
   }
   return run_raster(ctx, spec, optics, raster, detect, results);
+}
+
+msf_status msf_tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
+  if (!ctx || !spec || spec->ctx != ctx) {
+    set_error("specimen does not belong to this context");
+    return MSF_ERR_ARG;
+  }
+  return tune(ctx, spec, out);
 }
 
 msf_status msf_run_md(msf_context* ctx, int32_t n_snapshots,

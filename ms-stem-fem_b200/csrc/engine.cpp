@@ -422,8 +422,9 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   col.py = static_cast<const char*>(spec->prop.p) + cbytes * g.nx;
   // the same kernels run_raster launches for slices after the first
   const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
-  const bool pipe_row = pipe_ok && (ctx->pipe & MSF_PIPE_ROW);
-  const bool pipe_col = pipe_ok && (ctx->pipe & MSF_PIPE_COL);
+  const int pipe = ctx->pipe_for(g.nx, g.ny);
+  const bool pipe_row = pipe_ok && (pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_ok && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
   MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
@@ -906,8 +907,9 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   const size_t cbytes = fp64 ? 16 : 8;
   const int S = P.S, n_seg = P.n_seg;
 
-  // batch of wavefields
-  int B = ctx->batch;
+  // batch of wavefields: the context's, the tuned one for this grid, or
+  // what half the free memory holds, at most 64
+  int B = ctx->batch_for(g.nx, g.ny);
   if (B <= 0) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -933,8 +935,9 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
 
   // persistent TMA-pipelined passes for FP32 grids they support
   const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
-  const bool pipe_row = pipe_ok && (ctx->pipe & MSF_PIPE_ROW);
-  const bool pipe_col = pipe_ok && (ctx->pipe & MSF_PIPE_COL);
+  const int pipe = ctx->pipe_for(g.nx, g.ny);
+  const bool pipe_row = pipe_ok && (pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_ok && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
   MSF_TRY(ctx->alloc(&d_err, sizeof(int)));

@@ -56,6 +56,23 @@ struct msf_context {
   int64_t h2d_bytes = 0, d2h_bytes = 0;
   cudaStream_t stream = nullptr;
   std::map<int, msf::DevBuf> tw64, tw32;  // twiddle tables per length
+  // autotuned launch tiling per grid (nx, ny): probes per launch and the
+  // pipelined-pass mask (msf_tune, or imported wisdom)
+  struct Tuned {
+    int batch = 0;
+    int pipe = 0;
+    double ns_per_probe_slice = 0;
+  };
+  std::map<std::pair<int, int>, Tuned> tuned;
+  int batch_for(int nx, int ny) const {
+    auto it = tuned.find({nx, ny});
+    return batch > 0 ? batch : it != tuned.end() ? it->second.batch : 0;
+  }
+  int pipe_for(int nx, int ny) const {
+    auto it = tuned.find({nx, ny});
+    return (pipe_env || it == tuned.end()) ? pipe : it->second.pipe;
+  }
+  bool pipe_env = false;  // MSF_PIPE given: it wins over tuning
   msf_status alloc(msf::DevBuf* b, size_t bytes);
   msf_status twiddles(int n, bool fp64, const void** out);
 };
@@ -165,4 +182,7 @@ msf_status mtf_stage(msf_context* ctx, const RasterPlan& P, bool fp64, const voi
 msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps, int samples,
                   const msf_optics* optics, const msf_raster* raster, const msf_detect* det,
                   msf_results* res);
+// Times the slice passes of `spec`'s grid at candidate tilings and records
+// the fastest in ctx->tuned (tune.cpp).
+msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out);
 }  // namespace msf

@@ -979,6 +979,32 @@ struct RunBuffers {
   }
 };
 
+// The analogue of the reference's FFTW wisdom file (tem.cpp:583-616,
+// 1748-1765): msf_wisdom_<Nx>x<Ny>_<fp32|fp64> in the working directory is
+// imported when it exists and holds a line for this grid and device model;
+// otherwise the launch tiling is measured (msf_tune) and the file written.
+// Skipped when --batch fixes the tiling.
+void apply_wisdom(const msf_grid& grid, msf_context* ctx, const msf_specimen* spec,
+                  const msf_options& o) {
+  if (o.batch > 0) return;
+  const std::string name = "msf_wisdom_" + std::to_string(grid.nx) + "x" +
+                           std::to_string(grid.ny) + (o.precision == MSF_FP32 ? "_fp32" : "_fp64");
+  std::ifstream in(name.c_str());
+  if (in.is_open()) {
+    std::stringstream text;
+    text << in.rdbuf();
+    int32_t n = 0;
+    if (msf_wisdom_import(ctx, text.str().c_str(), &n) == MSF_OK && n > 0) return;
+  }
+  msf_tuning t;
+  if (msf_tune(ctx, spec, &t) != MSF_OK) return;  // the untuned defaults still run
+  const int64_t len = msf_wisdom_export(ctx, nullptr, 0);
+  std::vector<char> buf((size_t)len + 1);
+  msf_wisdom_export(ctx, buf.data(), len + 1);
+  std::ofstream out(name.c_str());
+  out << buf.data();
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- C ABI ------
@@ -1263,6 +1289,7 @@ int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) 
   int rc = 1;
   if ((st = msf_context_create(&o, &ctx)) == MSF_OK &&
       (st = msf_specimen_create(ctx, &grid, &atoms, &spec)) == MSF_OK) {
+    apply_wisdom(grid, ctx, spec, o);
     RunBuffers b;
     b.setup(j, grid, raster, det, true);
     if ((st = msf_run(ctx, spec, &optics, &raster, &det, &b.r)) == MSF_OK &&
@@ -1358,6 +1385,7 @@ int32_t msf_md_main(int32_t argc, const char* const* argv, const msf_options* op
       if ((st = msf_specimen_create(ctx, &gk, &a, &specs[k])) != MSF_OK) ok = false;
     }
     if (ok) {
+      apply_wisdom(grid, ctx, specs[0], o);
       RunBuffers b;
       b.setup(j, grid, raster, det, false);
       if ((st = msf_run_md(ctx, (int32_t)specs.size(), specs.data(),

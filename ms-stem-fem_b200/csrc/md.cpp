@@ -107,7 +107,7 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
   const int n_seg = A.n_seg, n_k = A.n_k;
 
   // batch: the wavefields, their FP64 average and (MTF) the filtered waves
-  int B = ctx->batch;
+  int B = ctx->batch_for(g.nx, g.ny);
   if (B <= 0) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -129,7 +129,8 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
   cudaStream_t st = ctx->stream;
   MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
 
-  const bool pipe_col = !fp64 && pipe_supported(g.nx, g.ny) && (ctx->pipe & MSF_PIPE_COL);
+  const bool pipe_col =
+      !fp64 && pipe_supported(g.nx, g.ny) && (ctx->pipe_for(g.nx, g.ny) & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map));
   PassArgs row, col;

@@ -45,11 +45,17 @@ EXPORTED = [
     "msf_run_batch", "msf_server_create", "msf_server_submit", "msf_server_poll",
     "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
     "msf_finish", "msf_run_plain", "msf_amorphous_positions", "msf_run_md", "msf_md_main",
+    "msf_tune", "msf_wisdom_export", "msf_wisdom_import",
 ]
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 _lp = C.POINTER(C.c_int64)
+
+
+class Tuning(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("batch", C.c_int32),
+                ("pipe", C.c_int32), ("ns_per_probe_slice", C.c_double)]
 
 
 class Options(C.Structure):
@@ -165,6 +171,10 @@ def lib() -> C.CDLL:
         L.msf_write_outputs.argtypes = [C.c_void_p, C.POINTER(Results)]
         L.msf_main.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(Options)]
         L.msf_md_main.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(Options)]
+        L.msf_tune.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Tuning)]
+        L.msf_wisdom_export.argtypes = [C.c_void_p, C.c_char_p, C.c_int64]
+        L.msf_wisdom_export.restype = C.c_int64
+        L.msf_wisdom_import.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]
         L.msf_run_md.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.c_int32,
                                  C.POINTER(Optics), C.POINTER(Raster), C.POINTER(Detect),
                                  C.POINTER(Results)]
@@ -315,6 +325,25 @@ class Context:
 
     def specimen(self, grid: Grid, q: np.ndarray, z: np.ndarray) -> "Specimen":
         return Specimen(self, grid, q, z)
+
+    def tune(self, spec: "Specimen") -> dict:
+        """Measure the launch tiling for the specimen's grid (msf_tune); the
+        context uses the winner for that grid from then on."""
+        t = Tuning()
+        _check(lib().msf_tune(self._h, spec._h, C.byref(t)))
+        return {"nx": t.nx, "ny": t.ny, "batch": t.batch, "pipe": t.pipe,
+                "ns_per_probe_slice": t.ns_per_probe_slice}
+
+    def wisdom_export(self) -> str:
+        n = lib().msf_wisdom_export(self._h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        lib().msf_wisdom_export(self._h, buf, n + 1)
+        return buf.value.decode()
+
+    def wisdom_import(self, text: str) -> int:
+        n = C.c_int32()
+        _check(lib().msf_wisdom_import(self._h, text.encode(), C.byref(n)))
+        return n.value
 
     def run(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
             want_final_psi=False, want_means=False, want_rings=False,

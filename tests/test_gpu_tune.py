@@ -1,0 +1,68 @@
+"""Launch tiling autotuner (msf_tune) and its wisdom text: the tuned tiling
+is one of the candidates, survives an export / import round trip on the same
+device model, is ignored for another model, and changes no result (a probe's
+arithmetic does not depend on its launch companions)."""
+import subprocess
+
+import numpy as np
+import pytest
+
+import msf
+from conftest import ROOT, case_dir, load_case
+from test_gpu_slots import JobSpec
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_tune_picks_a_candidate_and_keeps_results(precision):
+    j = JobSpec(256, 25.0, 14.0, 400, seed=51, raster_n=6)
+    ctx = msf.Context(precision=precision)
+    spec = ctx.specimen(j.grid, j.pos, j.z)
+    before = ctx.run(spec, j.optics, j.raster, j.detect)
+    t = ctx.tune(spec)
+    assert (t["nx"], t["ny"]) == (256, 256)
+    assert t["batch"] in (8, 16, 32, 64, 128, 256)
+    assert t["pipe"] in (0, 1) and t["ns_per_probe_slice"] > 0
+    if precision == "fp64":
+        assert t["pipe"] == 0 or t["pipe"] == ctx_pipe_default()
+    after = ctx.run(spec, j.optics, j.raster, j.detect)
+    assert np.array_equal(after.adf_image, before.adf_image)
+    for m in ("V_omega", "Vbar_r"):
+        assert np.array_equal(after.v[m], before.v[m], equal_nan=True), m
+    for m in ("V_re", "V_gt17"):
+        np.testing.assert_allclose(after.v[m], before.v[m], rtol=1e-12, equal_nan=True)
+
+
+def ctx_pipe_default():
+    return 1  # MSF_PIPE_COL
+
+
+def test_wisdom_round_trip():
+    j = JobSpec(128, 12.5, 10.0, 80, seed=52, raster_n=3)
+    ctx = msf.Context(precision="fp32")
+    spec = ctx.specimen(j.grid, j.pos, j.z)
+    t = ctx.tune(spec)
+    text = ctx.wisdom_export()
+    lines = text.strip().splitlines()
+    assert len(lines) == 1 and lines[0].startswith("msf-wisdom 1 ")
+    f = lines[0].split()
+    assert f[3] == "fp32" and (int(f[4]), int(f[5]), int(f[6])) == (128, 128, t["batch"])
+    other = msf.Context(precision="fp32")
+    assert other.wisdom_import(text) == 1
+    assert other.wisdom_export().split()[:8] == f[:8]
+    f2 = list(f)
+    f2[2] = "not_this_gpu"
+    assert msf.Context(precision="fp32").wisdom_import(" ".join(f2) + "\n") == 0
+    assert msf.Context(precision="fp64").wisdom_import(text) == 0
+
+
+def test_cli_writes_and_reuses_wisdom(golden_tmp, tmp_path):
+    meta, _ = load_case("fem128")
+    d = case_dir("fem128", tmp_path)
+    cli = ROOT / "ms-stem-fem_b200" / "bin" / "ms-stem-fem"
+    for _ in range(2):
+        p = subprocess.run([str(cli)] + meta["argv"], cwd=d, capture_output=True, text=True)
+        assert p.returncode == 0, p.stdout + p.stderr
+        w = (d / "msf_wisdom_128x128_fp64").read_text()
+        assert w.startswith("msf-wisdom 1 ") and " fp64 128 128 " in w
