@@ -100,6 +100,11 @@ msf_status msf_context_destroy(msf_context* ctx) {
   cudaStreamSynchronize(ctx->stream);
   ctx->tw64.clear();
   ctx->tw32.clear();
+  {  // buffers released after this point free their memory directly
+    std::lock_guard<std::mutex> lock(ctx->pool->m);
+    ctx->pool->closed = true;
+  }
+  ctx->pool->trim();
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return MSF_OK;

@@ -10,6 +10,7 @@
 // then finished on the host in FP64 in the reference's order
 // (adfstem.cpp:2489-3612).
 #include "engine.hpp"
+#include "trace.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -59,14 +60,46 @@ msf_status upload(msf_context* ctx, DevBuf* b, const std::vector<T>& h) {
 void set_error(const std::string& msg) { g_error = msg; }
 const char* last_error() { return g_error.c_str(); }
 
+void* Pool::take(size_t bytes, size_t* got) {
+  std::lock_guard<std::mutex> lock(m);
+  auto it = blocks.lower_bound(bytes);
+  if (it == blocks.end() || it->first > 2 * bytes + (4u << 20)) return nullptr;
+  void* p = it->second;
+  *got = it->first;
+  cached -= (int64_t)it->first;
+  blocks.erase(it);
+  return p;
+}
+
+void Pool::give(void* p, size_t bytes) {
+  cudaDeviceSynchronize();
+  std::lock_guard<std::mutex> lock(m);
+  live -= (int64_t)bytes;
+  if (closed) {
+    cudaFree(p);
+    return;
+  }
+  blocks.emplace(bytes, p);
+  cached += (int64_t)bytes;
+}
+
+void Pool::trim() {
+  std::lock_guard<std::mutex> lock(m);
+  for (auto& kv : blocks) cudaFree(kv.second);
+  blocks.clear();
+  cached = 0;
+}
+
 void DevBuf::release() {
   if (p) {
-    cudaFree(p);
-    if (counter) *counter -= (int64_t)bytes;
+    if (pool)
+      pool->give(p, bytes);
+    else
+      cudaFree(p);
   }
   p = nullptr;
   bytes = 0;
-  counter = nullptr;
+  pool.reset();
 }
 
 }  // namespace msf
@@ -75,20 +108,32 @@ using namespace msf;
 
 msf_status msf_context::alloc(DevBuf* b, size_t bytes) {
   b->release();
-  if (budget > 0 && allocated + (int64_t)bytes > budget) {
+  if (budget > 0 && pool->live + (int64_t)bytes > budget) {
     set_error("device allocation of " + std::to_string(bytes) +
               " bytes exceeds the context's HBM budget");
     return MSF_ERR_NOMEM;
   }
-  cudaError_t e = cudaMalloc(&b->p, bytes);
-  if (e != cudaSuccess) {
-    b->p = nullptr;
-    set_error(std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
-    return MSF_ERR_NOMEM;
+  size_t got = 0;
+  void* p = pool->take(bytes, &got);
+  if (!p) {
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {  // hand the cached blocks back and try once more
+      cudaGetLastError();
+      pool->trim();
+      e = cudaMalloc(&p, bytes);
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+      return MSF_ERR_NOMEM;
+    }
+    got = bytes;
   }
-  b->bytes = bytes;
-  b->counter = &allocated;
-  allocated += (int64_t)bytes;
+  b->p = p;
+  b->bytes = got;
+  b->pool = pool;
+  std::lock_guard<std::mutex> lock(pool->m);
+  pool->live += (int64_t)got;
   return MSF_OK;
 }
 
@@ -150,6 +195,7 @@ constexpr int64_t kPotentialFftAtoms = 64;
 
 msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms* atoms,
                           msf_specimen* spec) {
+  TraceScope trace_scope("specimen_build");
   const double t0 = now_s();
   if (!gin || !atoms) { set_error("null grid or atoms"); return MSF_ERR_ARG; }
   if (!grid_ok(gin->nx) || !grid_ok(gin->ny)) {
@@ -362,6 +408,7 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
 
 msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_optics* o,
                        DevBuf* probe64) {
+  TraceScope trace_scope("probe_build");
   const Grid& g = spec->g;
   const int64_t plane = (int64_t)g.nx * g.ny;
   MSF_TRY(ctx->alloc(probe64, 16 * plane));
@@ -388,6 +435,7 @@ msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_opt
 
 msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int reps,
                        double* ms_row, double* ms_col) {
+  TraceScope trace_scope("time_passes");
   const Grid& g = spec->g;
   const int64_t plane = (int64_t)g.nx * g.ny;
   const bool fp64 = ctx->fp64;
@@ -485,6 +533,7 @@ int64_t raster_plan_bytes(const msf_specimen* spec, bool fp64, int64_t n_probes,
 msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                        const msf_raster* raster, const msf_detect* det, RasterPlan* P,
                        int64_t p_begin, int64_t p_end) {
+  TraceScope trace_scope("raster_plan");
   if (!spec || !optics || !raster || !det || !P) { set_error("null argument"); return MSF_ERR_ARG; }
   const Grid& g = spec->g;
   const int64_t plane = (int64_t)g.nx * g.ny;
@@ -739,6 +788,7 @@ msf_status download_sums(msf_context* ctx, const RasterPlan& P, cudaStream_t str
 
 msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t stream,
                          msf_results* res) {
+  TraceScope trace_scope("raster_finish");
   std::vector<double> amp((size_t)P.n_probes * P.n_seg), inten((size_t)P.n_probes * P.n_seg);
   std::vector<double> acc_a, acc_i;
   if (P.pix_modes) {
@@ -900,6 +950,7 @@ msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& opti
 // the device.  Fills the timing / count fields of `res` and, when asked,
 // final_psi (the plan's last probe).
 msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) {
+  TraceScope trace_scope("raster_passes");
   const msf_specimen* spec = P.spec;
   const Grid& g = spec->g;
   const int64_t plane = P.plane, n_probes = P.n_probes;
@@ -1139,6 +1190,7 @@ msf_status run_raster(msf_context* ctx, const msf_specimen* spec, const msf_opti
 msf_status run_raster_plain(msf_context* ctx, const msf_specimen* spec,
                             const msf_optics* optics, const msf_raster* raster,
                             const msf_detect* det, msf_results* res) {
+  TraceScope trace_scope("raster_plain");
   if (!spec || !optics || !raster || !det || !res) { set_error("null argument"); return MSF_ERR_ARG; }
   if (!ctx->fp64) {
     set_error("the plain per-pass path runs FP64 wavefields: use an MSF_FP64 context");
@@ -1254,6 +1306,7 @@ msf_status run_partial(msf_context* ctx, const msf_specimen* spec, const msf_opt
                        const msf_raster* raster, const msf_detect* det, int64_t p_begin,
                        int64_t p_end, double* amp, double* inten, double* acc_a,
                        double* acc_i, msf_results* info) {
+  TraceScope trace_scope("raster_partial");
   if (!spec || !optics || !raster || !det) { set_error("null argument"); return MSF_ERR_ARG; }
   RasterPlan P;
   MSF_TRY(plan_raster(ctx, spec, optics, raster, det, &P, p_begin, p_end));

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -15,19 +16,40 @@ namespace msf {
 
 void set_error(const std::string& msg);
 
+// Device memory of one context.  `live` bytes count against the context's
+// budget; released blocks are kept for reuse by later allocations of about
+// their size (a new specimen, raster or request then maps no new memory),
+// and handed back to the driver when an allocation fails or the context
+// goes away.  Shared by the context and its buffers, so a buffer released
+// after its context frees its memory directly.
+struct Pool {
+  int64_t live = 0, cached = 0;
+  bool closed = false;
+  std::multimap<size_t, void*> blocks;
+  std::mutex m;
+  // A cached block of at least `bytes` and at most twice that (+4 MiB), or
+  // nullptr; *got receives its size.
+  void* take(size_t bytes, size_t* got);
+  // Keeps a released block.  Waits for the device first, as cudaFree does,
+  // so that no kernel still in flight on any stream can see it reused.
+  void give(void* p, size_t bytes);
+  void trim();  // cudaFree of every cached block
+  ~Pool() { trim(); }
+};
+
 // Owning device allocation that counts against its context's budget.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
-  int64_t* counter = nullptr;
+  std::shared_ptr<Pool> pool;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
   DevBuf& operator=(DevBuf&& o) noexcept {
     release();
-    p = o.p; bytes = o.bytes; counter = o.counter;
-    o.p = nullptr; o.bytes = 0; o.counter = nullptr;
+    p = o.p; bytes = o.bytes; pool = std::move(o.pool);
+    o.p = nullptr; o.bytes = 0; o.pool.reset();
     return *this;
   }
   ~DevBuf() { release(); }
@@ -52,7 +74,8 @@ struct msf_context {
   // direct / fft)
   int potential = 0;
   int64_t budget = 0;
-  int64_t allocated = 0;
+  std::shared_ptr<msf::Pool> pool = std::make_shared<msf::Pool>();
+  int64_t allocated() const { return pool->live; }
   int64_t h2d_bytes = 0, d2h_bytes = 0;
   cudaStream_t stream = nullptr;
   std::map<int, msf::DevBuf> tw64, tw32;  // twiddle tables per length

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "trace.hpp"
 #include "kernels.h"
 
 namespace msf {
@@ -65,6 +66,7 @@ bool same_cell(const Grid& a, const Grid& b) {
 msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps, int samples,
                   const msf_optics* optics, const msf_raster* raster, const msf_detect* det,
                   msf_results* res) {
+  TraceScope trace_scope("md_raster");
   if (!ctx || !snaps || !optics || !raster || !det || !res) {
     set_error("null argument");
     return MSF_ERR_ARG;

@@ -223,7 +223,7 @@ struct msf_server {
           std::unique_lock<std::mutex> lk(mu);
           if (waiting.empty()) break;
           const int64_t need = estimate_bytes(waiting.front());
-          if (!running.empty() && ctx->allocated + need > budget) break;
+          if (!running.empty() && ctx->allocated() + need > budget) break;
           r = std::move(waiting.front());
           waiting.pop_front();
           ++running_n;
@@ -284,14 +284,14 @@ struct msf_server {
           running.erase(running.begin() + i);
           std::lock_guard<std::mutex> lk(mu);
           --running_n;
-          held_bytes = ctx->allocated;
+          held_bytes = ctx->allocated();
           continue;
         }
         ++i;
       }
       {
         std::unique_lock<std::mutex> lk(mu);
-        held_bytes = ctx->allocated;
+        held_bytes = ctx->allocated();
         if (stopping && waiting.empty() && running.empty()) break;
         if (!worked) {
           if (running.empty() && waiting.empty())

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "trace.hpp"
 #include "kernels.h"
 
 namespace msf {
@@ -31,6 +32,7 @@ std::string device_tag(int device) {
 }  // namespace
 
 msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
+  TraceScope trace_scope("tune");
   const Grid& g = spec->g;
   const int64_t plane = (int64_t)g.nx * g.ny;
   const size_t cbytes = ctx->fp64 ? 16 : 8;
