@@ -94,6 +94,7 @@ FILES = {
     "mtf": {"mtf.param": "mtf_file mtf.csv\nmtf_sampling_rate 20\n",
             "mtf.csv": "0, 0.25, 0.5, 0.75, 1.0, 1.5\n1.0, 0.8, 0.55, 0.35, 0.2, 0.1\n"},
 }
+FILES["md_mtf"] = FILES["mtf"]
 
 
 def write_xyz(path, pos, box):
@@ -203,6 +204,12 @@ MD_CASES = {
            "-m 128 128 200000 --adfstemuncorrfem " + " ".join(FEM_ALL) +
            " --cs3 1.3e7 --scherzer_defocus --alphamax 0.010 --rasterspacing 6.25 "
            "--minslice 2.0 --images", 10, 6),
+    # detector MTF (parameter file) and the correlograph on the averaged wave
+    "md_mtf": (dict(n=780, box=(25, 25, 25), seed=1), (0.0, 0.0, 0.0), 2, 0.2, 43,
+               "--parameter_file mtf.param -m 128 128 200000 --adfstemuncorrfem --V_omega "
+               "--V_re --Omega_vimage --correlograph --correlograph_variance --cs3 1.3e7 "
+               "--scherzer_defocus --alphamax 0.010 --rasterspacing 8.333 --minslice 2.0 "
+               "--dr 1.0 --images", 5, 4),
     # no MD steps: every sample sees the initial configuration
     "md_static": (dict(n=390, box=(25, 25, 12.5), seed=11), (0.0, 0.0, 0.0), 0, 0.0, 0,
                   "-m 128 64 200000 --adfstemuncorrfem --V_omega --Vbar_r --cs3 1.3e7 "
@@ -243,6 +250,7 @@ def run_md_case(name):
         files[f] = (work / f).read_text()
         replay.append(f)
     files[name + ".in"] = PRE_TEM.format(initial=initial)
+    files.update(FILES.get(name, {}))
     if replay:
         files[name + "_replay.txt"] = "\n".join(replay) + "\n"
     for f, text in files.items():
@@ -261,6 +269,8 @@ def run_md_case(name):
     for tag in ("final", "diffracted_wave_avg", "diffracted_wave_sqr_avg", "variance_2-D"):
         for f in work.glob("%s_%s_diffraction_scalefactor_*.tif" % (name, tag)):
             out["%s_diffraction_%s" % (tag, f.stem.split("_scalefactor_")[1])] = read_tif16(f)
+    for f in sorted(work.glob(name + "_correlograph_*.txt")):
+        out["correlograph_" + f.stem.split("_correlograph_")[1]] = np.loadtxt(f, ndmin=2)
     np.savez_compressed(HERE / (name + ".npz"), **out)
     extra = ["--md_replay", name + "_replay.txt"] if replay else []
     meta = dict(case=name, argv=argv, md_argv_extra=extra, recipe=recipe, origin=origin,

@@ -45,6 +45,15 @@ def test_md_cli_matches_reference(name, precision, golden_tmp, tmp_path):
             np.testing.assert_allclose(t[:, 0], ref[mode][:, 0], rtol=1e-9)
             assert_variance_close(t[:, 1], ref[mode][:, 1], v_rtol, v_atol,
                                   what="%s %s %s" % (name, precision, mode))
+    crtol, catol = {"fp64": (1e-8, 1e-9), "fp32": (1e-4, 1e-5)}[precision]
+    for key, scale in (("correlograph_avg", 1), ("correlograph_variance", 2)):
+        if key in ref:
+            t = np.loadtxt(d / (meta["prefix"] + "_" + key + ".txt"), ndmin=2)
+            want = ref[key]
+            assert t.shape == want.shape, key
+            np.testing.assert_array_equal(t[0], want[0])  # phi boundaries
+            err = np.abs(t[1:, 1:] - want[1:, 1:])
+            assert (err <= scale * crtol * np.abs(want[1:, 1:]) + scale * 10 * catol).all(), key
     if precision == "fp64":
         keys = [k for k in ref if "_diffraction_" in k]
         assert keys

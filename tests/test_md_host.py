@@ -21,7 +21,7 @@ CLI = ROOT / "ms-stem-fem_b200" / "bin" / "ms-stem-fem"
 
 
 def test_md_cases_present():
-    assert golden_cases(md=True) == ["md", "md_static"]
+    assert golden_cases(md=True) == ["md", "md_mtf", "md_static"]
 
 
 def plain_argv(meta):
