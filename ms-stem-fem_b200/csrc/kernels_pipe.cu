@@ -179,7 +179,14 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
 }
 
 // ----------------------------------------------------- column slice pass --
-constexpr int ctas_per_256(int threads) { return threads >= 256 ? 1 : 256 / threads; }
+// Resident CTAs per SM the register allocator must allow: at least
+// MSF_COL_PIPE_THREADS_PER_SM threads of the pass per SM.
+#ifndef MSF_COL_PIPE_THREADS_PER_SM
+#define MSF_COL_PIPE_THREADS_PER_SM 256
+#endif
+constexpr int ctas_per_256(int threads) {
+  return threads >= MSF_COL_PIPE_THREADS_PER_SM ? 1 : MSF_COL_PIPE_THREADS_PER_SM / threads;
+}
 
 // SLOTS: every probe of the batch brings its own mask, propagator and step
 // (PassArgs::slots); LAST is then taken per probe from its slot.
