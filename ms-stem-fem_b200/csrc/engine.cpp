@@ -71,7 +71,13 @@ void* Pool::take(size_t bytes, size_t* got) {
   return p;
 }
 
+std::recursive_mutex& capture_mutex() {
+  static std::recursive_mutex m;
+  return m;
+}
+
 void Pool::give(void* p, size_t bytes) {
+  std::lock_guard<std::recursive_mutex> cap(capture_mutex());
   cudaDeviceSynchronize();
   std::lock_guard<std::mutex> lock(m);
   live -= (int64_t)bytes;
@@ -84,6 +90,7 @@ void Pool::give(void* p, size_t bytes) {
 }
 
 void Pool::trim() {
+  std::lock_guard<std::recursive_mutex> cap(capture_mutex());
   std::lock_guard<std::mutex> lock(m);
   for (auto& kv : blocks) cudaFree(kv.second);
   blocks.clear();
@@ -92,10 +99,12 @@ void Pool::trim() {
 
 void DevBuf::release() {
   if (p) {
-    if (pool)
+    if (pool) {
       pool->give(p, bytes);
-    else
+    } else {
+      std::lock_guard<std::recursive_mutex> cap(capture_mutex());
       cudaFree(p);
+    }
   }
   p = nullptr;
   bytes = 0;
@@ -1079,6 +1088,7 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
       MSF_CUDA(cudaMemcpyAsync(stage_shift.p, P.d_shifts.as<int32_t>() + 2 * p0,
                                sizeof(int32_t) * 2 * nb, cudaMemcpyDeviceToDevice, ctx->stream));
       if (!graph_exec) {
+        std::lock_guard<std::recursive_mutex> cap(capture_mutex());
         cudaGraph_t graph;
         MSF_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         st = enqueue_batch(nb, stage_shift.as<int32_t>(), stage_amp.as<double>(),

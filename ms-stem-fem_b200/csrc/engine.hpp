@@ -16,6 +16,12 @@ namespace msf {
 
 void set_error(const std::string& msg);
 
+// Held while a thread captures a CUDA graph and while a thread waits for the
+// whole device (cudaDeviceSynchronize, cudaFree): a device-wide wait from
+// one thread would invalidate another thread's capture (the serving loop's
+// builder and worker threads).
+std::recursive_mutex& capture_mutex();
+
 // Device memory of one context.  `live` bytes count against the context's
 // budget; released blocks are kept for reuse by later allocations of about
 // their size (a new specimen, raster or request then maps no new memory),

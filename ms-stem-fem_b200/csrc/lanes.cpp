@@ -132,6 +132,7 @@ msf_status Lane::launch_detect() {
 namespace {
 template <typename F>
 msf_status capture_graph(cudaStream_t stream, F&& enqueue, cudaGraphExec_t* out) {
+  std::lock_guard<std::recursive_mutex> cap(capture_mutex());
   cudaGraph_t graph;
   MSF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
   msf_status st = enqueue();

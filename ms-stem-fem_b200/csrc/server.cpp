@@ -1,18 +1,21 @@
 // msf_server: a request loop with continuous batching over slot lanes.
 //
-// Submission copies the request into a FIFO and returns a ticket.  One
-// worker thread owns the CUDA context and loops:
+// Submission copies the request into a FIFO and returns a ticket.  A worker
+// thread owns the lanes and loops:
 //   1. admit waiting requests in arrival order while their estimated device
 //      bytes fit the budget (the oldest is always admitted when nothing
-//      runs): build the specimen and the raster plan, hand its probes to the
-//      lane of its grid size (created on first use);
-//   2. step every lane that has work and a free table in its ring (no
+//      runs or builds) and hand them to the builder thread;
+//   2. hand the probes of every request the builder finished to the lane of
+//      its grid size (created on first use);
+//   3. step every lane that has work and a free table in its ring (no
 //      blocking, so a lane of small grids is not paced by a lane of large
 //      ones; the lanes' streams overlap on the GPU);
-//   3. finish the rasters whose completion event has fired (FEM statistics
+//   4. finish the rasters whose completion event has fired (FEM statistics
 //      on the host), publish their results and latency, free their memory.
-// A request that arrives while others run joins the running launches as soon
-// as slots of its grid size free up.
+// The builder thread builds specimens and raster plans on a context and
+// stream of its own, so those set-up kernels overlap the lanes' steps
+// instead of holding the worker.  A request that arrives while others run
+// joins the running launches as soon as slots of its grid size free up.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -68,6 +71,15 @@ struct Running {
   double setup_s = 0;
 };
 
+// A request between admission and its lane: built on the builder thread.
+struct Pending {
+  Request r;
+  Running run;
+  int64_t need = 0;  // estimated device bytes, held against the budget
+  msf_status status = MSF_OK;
+  std::string error;
+};
+
 int64_t estimate_bytes(const Request& r) {
   const int64_t plane = (int64_t)r.grid.nx * r.grid.ny;
   double zlo = 0, zhi = 0;
@@ -92,7 +104,12 @@ using namespace msf;
 
 struct msf_server {
   msf_options opt{};
-  msf_context* ctx = nullptr;
+  msf_context* ctx = nullptr;   // lanes (worker thread)
+  msf_context* bctx = nullptr;  // specimens and raster plans (builder thread)
+  std::thread builder;
+  std::condition_variable cv_build;
+  std::deque<Pending> to_build, built;  // guarded by mu
+  int64_t building_bytes = 0;
   int slots = 0;  // per lane; 0: by grid size (lane_slots)
   int64_t budget = 0;
   std::thread worker;
@@ -125,7 +142,9 @@ struct msf_server {
     cv_done.notify_all();
   }
 
-  msf_status admit(Request& r, Running* out) {
+  // Builder thread: the specimen and the raster plan, on bctx's stream
+  // (both end synchronised, so the lanes may read them at once).
+  msf_status build(Request& r, Running* out) {
     out->ticket = r.ticket;
     out->t_submit = r.t_submit;
     out->t_admit = now_s();
@@ -134,11 +153,10 @@ struct msf_server {
     atoms.q = r.q.data();
     atoms.z = r.z.data();
     out->spec = std::make_unique<msf_specimen>();
-    msf_status st = build_specimen(ctx, &r.grid, &atoms, out->spec.get());
+    msf_status st = build_specimen(bctx, &r.grid, &atoms, out->spec.get());
     if (st != MSF_OK) return st;
     out->setup_s = out->spec->seconds_setup;
     out->job = std::make_unique<SlotJob>();
-    out->job->order = order++;
     msf_raster raster;
     raster.n_x = (int32_t)r.xp.size();
     raster.n_y = (int32_t)r.yp.size();
@@ -146,8 +164,35 @@ struct msf_server {
     raster.y_p = r.yp.data();
     r.det.mtf = r.mtf.empty() ? nullptr : r.mtf.data();
     r.det.mtf_domain_sqr = r.mtf_domain_sqr.empty() ? nullptr : r.mtf_domain_sqr.data();
-    st = plan_raster(ctx, out->spec.get(), &r.optics, &raster, &r.det, &out->job->plan);
-    if (st != MSF_OK) return st;
+    return plan_raster(bctx, out->spec.get(), &r.optics, &raster, &r.det, &out->job->plan);
+  }
+
+  void build_loop() {
+    cudaSetDevice(bctx->device);
+    for (;;) {
+      Pending p;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_build.wait(lk, [&] { return stopping_builder || !to_build.empty(); });
+        if (to_build.empty()) return;
+        p = std::move(to_build.front());
+        to_build.pop_front();
+      }
+      p.status = build(p.r, &p.run);
+      if (p.status != MSF_OK) p.error = last_error_copy();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        built.push_back(std::move(p));
+      }
+      cv_work.notify_one();
+    }
+  }
+  bool stopping_builder = false;
+
+  // Worker thread: a built request joins the lane of its grid size.
+  msf_status join_lane(const Request& r, Running* out) {
+    out->job->order = order++;
+    msf_status st;
     const std::pair<int, int> key{r.grid.nx, r.grid.ny};
     auto it = lanes.find(key);
     if (it == lanes.end()) {
@@ -216,36 +261,53 @@ struct msf_server {
     cudaSetDevice(ctx->device);
     for (;;) {
       bool worked = false;
-      // 1. admission
-      for (;;) {
-        Request r;
-        {
-          std::unique_lock<std::mutex> lk(mu);
-          if (waiting.empty()) break;
+      // 1. admission: to the builder
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        while (!waiting.empty()) {
           const int64_t need = estimate_bytes(waiting.front());
-          if (!running.empty() && ctx->allocated() + need > budget) break;
-          r = std::move(waiting.front());
+          const bool idle = running.empty() && to_build.empty() && built.empty();
+          if (!idle && ctx->allocated() + bctx->allocated() + building_bytes + need > budget)
+            break;
+          Pending p;
+          p.r = std::move(waiting.front());
+          p.need = need;
           waiting.pop_front();
           ++running_n;
+          building_bytes += need;
+          to_build.push_back(std::move(p));
+          cv_build.notify_one();
+          worked = true;
         }
-        Running run;
-        msf_status st = admit(r, &run);
+      }
+      // 2. built requests join their lanes
+      for (;;) {
+        Pending p;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          if (built.empty()) break;
+          p = std::move(built.front());
+          built.pop_front();
+          building_bytes -= p.need;
+        }
         worked = true;
+        msf_status st = p.status;
+        if (st == MSF_OK) st = join_lane(p.r, &p.run);
         if (st != MSF_OK) {
           Stored s;
           s.status = st;
-          s.error = last_error_copy();
-          s.latency = now_s() - r.t_submit;
+          s.error = p.status != MSF_OK ? p.error : last_error_copy();
+          s.latency = now_s() - p.r.t_submit;
           {
             std::lock_guard<std::mutex> lk(mu);
             --running_n;
           }
-          publish(r.ticket, std::move(s));
+          publish(p.r.ticket, std::move(s));
           continue;
         }
-        running.push_back(std::move(run));
+        running.push_back(std::move(p.run));
       }
-      // 2. one step of every lane that can take one without waiting
+      // 3. one step of every lane that can take one without waiting
       for (auto it = lanes.begin(); it != lanes.end();) {
         Lane* lane = it->second.get();
         if (!lane->busy() || !lane->ready()) {
@@ -272,7 +334,7 @@ struct msf_server {
             r.job.reset();
           }
       }
-      // 3. completions
+      // 4. completions
       for (size_t i = 0; i < running.size();) {
         Running& r = running[i];
         const bool gone = !r.job;
@@ -284,17 +346,19 @@ struct msf_server {
           running.erase(running.begin() + i);
           std::lock_guard<std::mutex> lk(mu);
           --running_n;
-          held_bytes = ctx->allocated();
+          held_bytes = ctx->allocated() + bctx->allocated();
           continue;
         }
         ++i;
       }
       {
         std::unique_lock<std::mutex> lk(mu);
-        held_bytes = ctx->allocated();
-        if (stopping && waiting.empty() && running.empty()) break;
+        held_bytes = ctx->allocated() + bctx->allocated();
+        const bool empty =
+            waiting.empty() && running.empty() && to_build.empty() && built.empty();
+        if (stopping && empty) break;
         if (!worked) {
-          if (running.empty() && waiting.empty())
+          if (empty)
             cv_work.wait_for(lk, std::chrono::milliseconds(50));
           else
             cv_work.wait_for(lk, std::chrono::microseconds(50));
@@ -322,6 +386,12 @@ msf_status msf_server_create(const msf_options* opt, int32_t slots, msf_server**
     delete s;
     return st;
   }
+  st = msf_context_create(&o, &s->bctx);
+  if (st != MSF_OK) {
+    msf_context_destroy(s->ctx);
+    delete s;
+    return st;
+  }
   s->slots = slots > 0 ? slots : 0;
   if (o.hbm_budget > 0) {
     s->budget = o.hbm_budget;
@@ -331,6 +401,8 @@ msf_status msf_server_create(const msf_options* opt, int32_t slots, msf_server**
     s->budget = (int64_t)(0.8 * (double)free_b);
   }
   s->ctx->budget = 0;  // admission enforces the budget; allocations may overshoot briefly
+  s->bctx->budget = 0;
+  s->builder = std::thread([s] { s->build_loop(); });
   s->worker = std::thread([s] { s->loop(); });
   *out = s;
   return MSF_OK;
@@ -465,9 +537,16 @@ msf_status msf_server_destroy(msf_server* s) {
   }
   s->cv_work.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping_builder = true;
+  }
+  s->cv_build.notify_all();
+  if (s->builder.joinable()) s->builder.join();
   s->running.clear();
   s->lanes.clear();
   msf_context_destroy(s->ctx);
+  msf_context_destroy(s->bctx);
   delete s;
   return MSF_OK;
 }
