@@ -314,7 +314,7 @@ typedef struct {
 } msf_request;
 
 typedef struct {
-  int64_t submitted, completed, failed, running, waiting;
+  int64_t submitted, completed, failed, running, waiting; /* failed: incl. cancelled */
   double p50_s, p99_s, max_s;  /* latency, submission to completion         */
   double probe_slices_per_s;   /* completed probe*slices / busy wall time    */
   int64_t probe_slices;
@@ -338,6 +338,12 @@ msf_status msf_server_submit(msf_server* srv, const msf_request* req, uint64_t* 
 msf_status msf_server_poll(msf_server* srv, uint64_t ticket, int32_t wait_ms,
                            msf_results* results);
 msf_status msf_server_stats_get(msf_server* srv, msf_server_stats* out);
+/* Cancels a request: one still waiting for admission is dropped at once;
+ * one already admitted runs to the end of its probes (they share launches
+ * with other requests) and its results are discarded; a finished one not
+ * yet polled loses its results.  Its poll then returns MSF_ERR_CANCELLED.
+ * MSF_ERR_ARG for an unknown, delivered or already cancelled ticket. */
+msf_status msf_server_cancel(msf_server* srv, uint64_t ticket);
 /* Finishes the running and queued requests, then stops the worker. */
 msf_status msf_server_destroy(msf_server* srv);
 

@@ -24,6 +24,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -119,6 +120,8 @@ struct msf_server {
   uint64_t next_ticket = 1;
   std::deque<Request> waiting;
   std::map<uint64_t, Stored> done;
+  std::set<uint64_t> cancelled;  // admitted requests whose results are discarded
+  std::set<uint64_t> live;       // submitted, not yet finished
   std::vector<double> latencies;
   int64_t submitted = 0, completed = 0, failed = 0, running_n = 0, probe_slices = 0;
   double t_first = -1, t_last = 0;
@@ -130,6 +133,12 @@ struct msf_server {
 
   void publish(uint64_t ticket, Stored&& s) {
     std::lock_guard<std::mutex> lk(mu);
+    live.erase(ticket);
+    if (cancelled.erase(ticket)) {
+      s = Stored();
+      s.status = MSF_ERR_CANCELLED;
+      s.error = "request " + std::to_string(ticket) + " was cancelled";
+    }
     if (s.status == MSF_OK) {
       ++completed;
       latencies.push_back(s.latency);
@@ -440,6 +449,7 @@ msf_status msf_server_submit(msf_server* s, const msf_request* req, uint64_t* ti
     r.ticket = s->next_ticket++;
     *ticket = r.ticket;
     ++s->submitted;
+    s->live.insert(r.ticket);
     if (s->t_first < 0) s->t_first = r.t_submit;
     s->waiting.push_back(std::move(r));
   }
@@ -526,6 +536,37 @@ msf_status msf_server_stats_get(msf_server* s, msf_server_stats* out) {
   if (s->t_first >= 0 && s->t_last > s->t_first)
     st.probe_slices_per_s = (double)s->probe_slices / (s->t_last - s->t_first);
   *out = st;
+  return MSF_OK;
+}
+
+msf_status msf_server_cancel(msf_server* s, uint64_t ticket) {
+  if (!s) return MSF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const std::string why = "request " + std::to_string(ticket) + " was cancelled";
+  auto fin = s->done.find(ticket);
+  if (fin != s->done.end() && fin->second.status == MSF_OK) {
+    fin->second = Stored();  // it ran (the statistics keep it); its results go
+    fin->second.status = MSF_ERR_CANCELLED;
+    fin->second.error = why;
+    return MSF_OK;
+  }
+  if (!s->live.count(ticket) || s->cancelled.count(ticket)) {
+    set_error("unknown, delivered or already cancelled ticket");
+    return MSF_ERR_ARG;
+  }
+  for (auto it = s->waiting.begin(); it != s->waiting.end(); ++it)
+    if (it->ticket == ticket) {
+      s->waiting.erase(it);
+      s->live.erase(ticket);
+      Stored d;
+      d.status = MSF_ERR_CANCELLED;
+      d.error = why;
+      ++s->failed;
+      s->done[ticket] = std::move(d);
+      s->cv_done.notify_all();
+      return MSF_OK;
+    }
+  s->cancelled.insert(ticket);  // admitted: discarded when it finishes
   return MSF_OK;
 }
 

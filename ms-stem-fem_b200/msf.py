@@ -45,7 +45,7 @@ EXPORTED = [
     "msf_run_batch", "msf_server_create", "msf_server_submit", "msf_server_poll",
     "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
     "msf_finish", "msf_run_plain", "msf_amorphous_positions", "msf_run_md", "msf_md_main",
-    "msf_tune", "msf_wisdom_export", "msf_wisdom_import",
+    "msf_tune", "msf_wisdom_export", "msf_wisdom_import", "msf_server_cancel",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -184,6 +184,7 @@ def lib() -> C.CDLL:
         L.msf_server_create.argtypes = [C.POINTER(Options), C.c_int32, C.POINTER(C.c_void_p)]
         L.msf_server_submit.argtypes = [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]
         L.msf_server_poll.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(Results)]
+        L.msf_server_cancel.argtypes = [C.c_void_p, C.c_uint64]
         L.msf_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         L.msf_server_destroy.argtypes = [C.c_void_p]
         L.msf_segment_count.argtypes = [C.POINTER(Grid), C.POINTER(Detect)]
@@ -510,6 +511,11 @@ class Server:
         _check(st)
         out.finish(raster, detect)
         return out
+
+    def cancel(self, ticket: int):
+        """Cancel a request (msf_server_cancel): its poll then raises
+        MsfError with status MSF_ERR_CANCELLED (9)."""
+        _check(lib().msf_server_cancel(self._h, C.c_uint64(ticket)))
 
     def stats(self) -> dict:
         s = ServerStats()

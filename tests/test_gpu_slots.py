@@ -140,3 +140,32 @@ def test_server_reports_request_errors():
     st = srv.stats()
     assert st["failed"] == 1 and st["completed"] == 1
     srv.close()
+
+
+def test_server_cancel():
+    """A cancelled request polls MSF_ERR_CANCELLED whether it was still
+    queued (a 1-byte budget keeps later requests waiting while one runs) or
+    already admitted; the other requests are not disturbed."""
+    js = jobs_mixed()
+    srv = msf.Server(slots=4, hbm_budget=1)
+    ta = srv.submit(js[3].grid, js[3].pos, js[3].z, js[3].optics, js[3].raster, js[3].detect)
+    tb = srv.submit(js[1].grid, js[1].pos, js[1].z, js[1].optics, js[1].raster, js[1].detect)
+    tc = srv.submit(js[4].grid, js[4].pos, js[4].z, js[4].optics, js[4].raster, js[4].detect)
+    srv.cancel(tc)  # queued behind ta
+    srv.cancel(ta)  # admitted (or about to be): runs, results discarded
+    for t in (ta, tc):
+        with pytest.raises(msf.MsfError) as e:
+            while srv.poll(t, wait_ms=200) is None:
+                pass
+        assert e.value.status == 9
+    r = None
+    while r is None:
+        r = srv.poll(tb, wait_ms=200)
+    assert r.probe_slices > 0
+    with pytest.raises(msf.MsfError):
+        srv.cancel(tb)  # delivered
+    with pytest.raises(msf.MsfError):
+        srv.cancel(10 ** 6)  # unknown
+    st = srv.stats()
+    assert st["completed"] == 1 and st["failed"] == 2
+    srv.close()

@@ -115,3 +115,53 @@ def test_segment_count_matches_ring_bins():
     assert msf.segment_count(g, d) == nk.value + 1
     adf_only = msf.Detect(outputs=msf.OUT_ADF_IMAGE, det_inner=0.04, det_outer=0.2, dr=1.0)
     assert msf.segment_count(g, adf_only) == 1
+
+
+def _dying_rank(rank, world, port, out_dir):
+    """Rank 1 dies between steps, before the exchange; rank 0 must get an
+    error from its collective within the process group's timeout."""
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=10))
+    g, o, d, r, keep = job()
+    n_seg = msf.segment_count(g, d)
+    plane = g.nx * g.ny
+    amp, inten, acc = synthetic_rows(n_seg, plane)
+    if rank == 1:
+        os._exit(3)
+    b, e = shards.probe_range(N_PROBES, rank, world)
+    part = {"amp": amp[b:e], "inten": inten[b:e], "acc_a": acc[rank, 0], "acc_i": acc[rank, 1]}
+    t0 = time.time()
+    try:
+        shards.exchange(part, N_PROBES, world, dist, "cpu", plane)
+        outcome = "no-error"
+    except Exception as ex:
+        outcome = "error:" + type(ex).__name__
+    with open(os.path.join(out_dir, "rank0.txt"), "w") as f:
+        f.write("%s %.1f\n" % (outcome, time.time() - t0))
+    os._exit(0)
+
+
+def test_rank_failure_surfaces_as_error_not_hang():
+    import multiprocessing as mpp
+    ctx = mpp.get_context("spawn")
+    with tempfile.TemporaryDirectory() as out:
+        port = free_port()
+        procs = [ctx.Process(target=_dying_rank, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=120)
+        alive = [p for p in procs if p.is_alive()]
+        for p in alive:
+            p.kill()
+        assert not alive, "a rank hung"
+        assert procs[1].exitcode == 3
+        outcome, seconds = open(os.path.join(out, "rank0.txt")).read().split()
+        assert outcome.startswith("error:"), outcome
+        assert float(seconds) < 60.0
