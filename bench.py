@@ -213,7 +213,9 @@ def run_reference_arm(args):
     cores = os.cpu_count() or 1
     vals = []
     sample = None
-    for _ in range(max(1, args.steps)):  # no warm-up: nothing to compile or cache
+    for _ in range(max(0, args.warmup)):  # page cache, process start-up, CPU clocks
+        reference_sample(cores, cap_seconds=300)
+    for _ in range(max(1, args.steps)):
         s = reference_sample(cores, cap_seconds=300)
         if s is None:
             print(json.dumps({"impl": "reference", "unavailable":
@@ -226,7 +228,7 @@ def run_reference_arm(args):
             break
     v = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
-            "n_gpus": args.gpus, "steps": len(vals), "warmup": 0,
+            "n_gpus": args.gpus, "steps": len(vals), "warmup": max(0, args.warmup),
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "FEM 1024^2 amorphous Si (bounded CPU sample)",
@@ -430,19 +432,24 @@ def run_serving(msf, local, n_jobs, rate, slots, seed=5):
             "max_s": round(st["max_s"], 3), "completed": st["completed"],
             "failed": st["failed"], "probe_slices": st["probe_slices"],
             "throughput": round(st["probe_slices"] / wall, 1), "unit": UNIT,
+            "offered": round(st["probe_slices"] / max(float(gaps.sum()), 1e-9), 1),
             "wall_s": round(wall, 2),
             "mix": {str(n): sum(1 for r in reqs if r["n"] == n) for n in (256, 512, 1024, 2048)}}
 
 
 def workload_serving(args, msf, local):
     s = run_serving(msf, local, args.jobs, args.rate, args.batch)
+    # the same stream at a rate one GPU sustains (offered load below
+    # capacity): latency is then service time plus a short queue
+    sustained = (run_serving(msf, local, args.sustained_jobs, args.sustained_rate, args.batch,
+                             seed=7) if args.sustained_jobs > 0 else None)
     line = {"metric": "serving p99 latency, Poisson arrivals, mixed 256^2-2048^2 requests",
             "value": s["p99_s"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
             "ms_per_step": None, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "request stream: grids 256..2048^2, rasters 8..64^2, "
                                    "5..30 nm thick, ADF or FEM, 50 atoms/nm^3"},
-            "serving": s}
+            "serving": s, "sustained": sustained}
     print(json.dumps(line))
     return 0
 
@@ -472,6 +479,10 @@ def main():
                          "Poisson request stream through msf_server")
     ap.add_argument("--jobs", type=int, default=24, help="requests of --workload serving")
     ap.add_argument("--rate", type=float, default=20.0, help="request arrivals per second")
+    ap.add_argument("--sustained-jobs", type=int, default=12,
+                    help="requests of the second --workload serving run, at --sustained-rate")
+    ap.add_argument("--sustained-rate", type=float, default=0.2,
+                    help="arrivals per second one GPU sustains for the mixed stream")
     ap.add_argument("--serving-jobs", type=int, default=8,
                     help="requests of the serving sample in the headline line (0: none)")
     args = ap.parse_args()
