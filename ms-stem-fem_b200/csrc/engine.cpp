@@ -478,21 +478,20 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   col.px = spec->prop.p;
   col.py = static_cast<const char*>(spec->prop.p) + cbytes * g.nx;
   // the same kernels run_raster launches for slices after the first
-  const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
   const int pipe = ctx->pipe_for(g.nx, g.ny);
-  const bool pipe_row = pipe_ok && (pipe & MSF_PIPE_ROW);
-  const bool pipe_col = pipe_ok && (pipe & MSF_PIPE_COL);
+  const bool pipe_row = !fp64 && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_supported(g.nx, g.ny, fp64) && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
   MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
   MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
-  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, nb, g.nx, g.ny, col_map));
+  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, nb, g.nx, g.ny, col_map, fp64));
   auto row_pass = [&]() {
     return pipe_row ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
                     : launch_row(fp64, rop, row, ctx->stream);
   };
   auto col_pass = [&]() {
-    return pipe_col ? launch_col_slice_pipe(col, false, col_map, d_err.as<int>(), ctx->stream)
+    return pipe_col ? launch_col_slice_pipe(col, false, col_map, d_err.as<int>(), ctx->stream, fp64)
                     : launch_col(fp64, COL_SLICE, col, ctx->stream);
   };
   std::vector<cudaEvent_t> ev(2 * reps + 2);
@@ -994,15 +993,14 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   seg.partial = d_partial.as<double>();
 
   // persistent TMA-pipelined passes for FP32 grids they support
-  const bool pipe_ok = !fp64 && pipe_supported(g.nx, g.ny);
   const int pipe = ctx->pipe_for(g.nx, g.ny);
-  const bool pipe_row = pipe_ok && (pipe & MSF_PIPE_ROW);
-  const bool pipe_col = pipe_ok && (pipe & MSF_PIPE_COL);
+  const bool pipe_row = !fp64 && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
+  const bool pipe_col = pipe_supported(g.nx, g.ny, fp64) && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
   MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
   MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
-  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map));
+  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map, fp64));
 
   PassArgs row, col;
   row.psi = col.psi = psi.p;
@@ -1041,7 +1039,8 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
       col.px = pbase + prop_stride * s;
       col.py = pbase + prop_stride * s + cbytes * g.nx;
       if (pipe_col)
-        MSF_CUDA(launch_col_slice_pipe(col, s + 1 == S, col_map, d_err.as<int>(), ctx->stream));
+        MSF_CUDA(launch_col_slice_pipe(col, s + 1 == S, col_map, d_err.as<int>(), ctx->stream,
+                                       fp64));
       else
         MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
     }

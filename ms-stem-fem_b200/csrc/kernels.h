@@ -92,9 +92,10 @@ bool supported_length(int n);
 cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s);
 cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s);
 
-// ---- persistent TMA-pipelined FP32 slice passes (kernels_pipe.cu) ----
-// Supported for FP32 grids with sides 256..2048.
-bool pipe_supported(int nx, int ny);
+// ---- persistent TMA-pipelined slice passes (kernels_pipe.cu) ----
+// The column pass: FP32 grids with sides 256..2048, FP64 grids with sides
+// 256..1024; the split-wave row pass: FP32 only.
+bool pipe_supported(int nx, int ny, bool fp64 = false);
 // Split-wave row pass for slices after the first; *err set to 1 if a copy
 // never arrived (bounded wait).
 cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s);
@@ -102,9 +103,10 @@ cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s);
 // when a.slots is set); `tensor_map` from encode_column_map over the same
 // batch buffer.
 cudaError_t launch_col_slice_pipe(const PassArgs& a, bool last, const void* tensor_map,
-                                  int* err, cudaStream_t s);
+                                  int* err, cudaStream_t s, bool fp64 = false);
 // Encode the 2-D tensor map (128 bytes) the column pass loads tiles with.
-cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out);
+cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out,
+                              bool fp64 = false);
 
 // Twiddle table e^{-2 pi i m / n}, m < n, computed in FP64 on the host.
 void fill_twiddles(int n, double* host_interleaved /* 2n */);

@@ -188,16 +188,19 @@ constexpr int ctas_per_256(int threads) {
   return threads >= MSF_COL_PIPE_THREADS_PER_SM ? 1 : MSF_COL_PIPE_THREADS_PER_SM / threads;
 }
 
-// SLOTS: every probe of the batch brings its own mask, propagator and step
-// (PassArgs::slots); LAST is then taken per probe from its slot.
-template <int N, int COLS, bool LAST, bool SLOTS>
-__global__ void __launch_bounds__(COLS * Shape<N, float>::T,
-                                  ctas_per_256(COLS * Shape<N, float>::T))
+// Real: float (the split-wave passes) or double (FP64 runs; a complex value
+// is then two 8-byte tensor-map elements).  SLOTS (FP32 only): every probe
+// of the batch brings its own mask, propagator and step (PassArgs::slots);
+// LAST is then taken per probe from its slot.
+template <typename Real, int N, int COLS, bool LAST, bool SLOTS>
+__global__ void __launch_bounds__(COLS * Shape<N, Real>::T,
+                                  ctas_per_256(COLS * Shape<N, Real>::T))
 col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap, int* err) {
-  using C = float2;
-  using Sh = Shape<N, float>;
-  using SM = Smem<Sh, 8, COLS, true>;
+  using C = Cx<Real>;
+  using Sh = Shape<N, Real>;
+  using SM = Smem<Sh, (int)sizeof(C), COLS, true>;
   constexpr int E = Sh::E, T = Sh::T;
+  constexpr int EPC = (int)sizeof(C) / 8;  // tensor-map elements per complex value
   constexpr int BOX = N < 256 ? N : 256;
   constexpr int RAW = (N * COLS > COLS * SM::stride ? N * COLS : COLS * SM::stride);
   constexpr int BUF = (RAW + 15) / 16 * 16;  // 128-byte multiple
@@ -211,10 +214,10 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
   auto issue = [&](int item, int which) {
     const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
     C* dst = bufs + which * BUF;
-    mbar_expect_tx(&bars[which], N * COLS * 8);
+    mbar_expect_tx(&bars[which], N * COLS * (int)sizeof(C));
 #pragma unroll
     for (int q = 0; q < N / BOX; ++q)
-      tile_g2s(dst + q * BOX * COLS, &tmap, g * COLS, b * a.nx + q * BOX, &bars[which]);
+      tile_g2s(dst + q * BOX * COLS, &tmap, g * COLS * EPC, b * a.nx + q * BOX, &bars[which]);
   };
   if (threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
@@ -229,7 +232,7 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
   }
   uint32_t parity[2] = {0, 0};
   const C* tw = static_cast<const C*>(a.tw);
-  const float is = (float)a.inv_s;
+  const Real is = (Real)a.inv_s;
   const C* px = static_cast<const C*>(a.px);
   int k = 0;
   for (; item < items; ++k, item += gridDim.x) {
@@ -278,7 +281,7 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
           const C p = cmul(__ldg(pxb + i), pyj);
           v[m] = cmul(p, cscale(v[m], is));
         } else {
-          v[m] = C{0.f, 0.f};
+          v[m] = C{Real(0), Real(0)};
         }
       }
       if (!stop_in_k) fft_line<Sh, true>(v, sm, t, tw, sync);
@@ -312,10 +315,10 @@ constexpr int pipe_lines() { return 256 / Shape<N, float>::T; }
 #ifndef MSF_COL_PIPE_THREADS
 #define MSF_COL_PIPE_THREADS 256
 #endif
-template <int N>
+template <typename Real, int N>
 constexpr int pipe_cols() {
   int c = 16;
-  while (c > 2 && c * Shape<N, float>::T > MSF_COL_PIPE_THREADS) c >>= 1;
+  while (c > 2 && c * Shape<N, Real>::T > MSF_COL_PIPE_THREADS) c >>= 1;
   return c;
 }
 
@@ -337,41 +340,53 @@ cudaError_t row_pipe_launch(const PassArgs& a, int* err, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int N, bool LAST, bool SLOTS = false>
+template <typename Real, int N, bool LAST, bool SLOTS = false>
 cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
                             cudaStream_t s) {
-  constexpr int CC = pipe_cols<N>();
-  using SM = Smem<Shape<N, float>, 8, CC, true>;
+  constexpr int CC = pipe_cols<Real, N>();
+  constexpr int CB = (int)sizeof(Cx<Real>);
+  using SM = Smem<Shape<N, Real>, CB, CC, true>;
   constexpr int RAW = (N * CC > CC * SM::stride ? N * CC : CC * SM::stride);
-  constexpr int smem = 2 * ((RAW + 15) / 16 * 16) * 8;
+  constexpr int smem = 2 * ((RAW + 15) / 16 * 16) * CB;
   static int per_sm = 0;
-  auto k = col_slice_pipe_kernel<N, CC, LAST, SLOTS>;
+  auto k = col_slice_pipe_kernel<Real, N, CC, LAST, SLOTS>;
   if (!per_sm) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, CC * Shape<N, float>::T, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, CC * Shape<N, Real>::T, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
   }
   const int items = a.nb * (a.ny / CC);
   const int grid = items < per_sm * sm_count() ? items : per_sm * sm_count();
-  k<<<grid, CC * Shape<N, float>::T, smem, s>>>(a, map, err);
+  k<<<grid, CC * Shape<N, Real>::T, smem, s>>>(a, map, err);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-bool pipe_supported(int nx, int ny) {
-  auto ok = [](int n) { return n == 256 || n == 512 || n == 1024 || n == 2048; };
+bool pipe_supported(int nx, int ny, bool fp64) {
+  // FP64 tiles of 2048-point columns would be 2 columns (32-byte rows) wide
+  auto ok = [fp64](int n) {
+    return n == 256 || n == 512 || n == 1024 || (!fp64 && n == 2048);
+  };
   return ok(nx) && ok(ny);
 }
 
-int pipe_cols_for(int nx) {
+int pipe_cols_for(int nx, bool fp64) {
+  if (fp64) {
+    switch (nx) {
+      case 256: return pipe_cols<double, 256>();
+      case 512: return pipe_cols<double, 512>();
+      case 1024: return pipe_cols<double, 1024>();
+    }
+    return 0;
+  }
   switch (nx) {
-    case 256: return pipe_cols<256>();
-    case 512: return pipe_cols<512>();
-    case 1024: return pipe_cols<1024>();
-    case 2048: return pipe_cols<2048>();
+    case 256: return pipe_cols<float, 256>();
+    case 512: return pipe_cols<float, 512>();
+    case 1024: return pipe_cols<float, 1024>();
+    case 2048: return pipe_cols<float, 2048>();
   }
   return 0;
 }
@@ -387,29 +402,39 @@ cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s) {
 }
 
 cudaError_t launch_col_slice_pipe(const PassArgs& a, bool last, const void* tensor_map,
-                                  int* err, cudaStream_t s) {
+                                  int* err, cudaStream_t s, bool fp64) {
   const CUtensorMap& m = *static_cast<const CUtensorMap*>(tensor_map);
+  if (fp64) {
+    if (a.slots) return cudaErrorInvalidValue;
+    switch (a.nx) {
+      case 256: return last ? col_pipe_launch<double, 256, true>(a, m, err, s) : col_pipe_launch<double, 256, false>(a, m, err, s);
+      case 512: return last ? col_pipe_launch<double, 512, true>(a, m, err, s) : col_pipe_launch<double, 512, false>(a, m, err, s);
+      case 1024: return last ? col_pipe_launch<double, 1024, true>(a, m, err, s) : col_pipe_launch<double, 1024, false>(a, m, err, s);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (a.slots) {
     switch (a.nx) {
-      case 256: return col_pipe_launch<256, false, true>(a, m, err, s);
-      case 512: return col_pipe_launch<512, false, true>(a, m, err, s);
-      case 1024: return col_pipe_launch<1024, false, true>(a, m, err, s);
-      case 2048: return col_pipe_launch<2048, false, true>(a, m, err, s);
+      case 256: return col_pipe_launch<float, 256, false, true>(a, m, err, s);
+      case 512: return col_pipe_launch<float, 512, false, true>(a, m, err, s);
+      case 1024: return col_pipe_launch<float, 1024, false, true>(a, m, err, s);
+      case 2048: return col_pipe_launch<float, 2048, false, true>(a, m, err, s);
     }
     return cudaErrorInvalidValue;
   }
   switch (a.nx) {
-    case 256: return last ? col_pipe_launch<256, true>(a, m, err, s) : col_pipe_launch<256, false>(a, m, err, s);
-    case 512: return last ? col_pipe_launch<512, true>(a, m, err, s) : col_pipe_launch<512, false>(a, m, err, s);
-    case 1024: return last ? col_pipe_launch<1024, true>(a, m, err, s) : col_pipe_launch<1024, false>(a, m, err, s);
-    case 2048: return last ? col_pipe_launch<2048, true>(a, m, err, s) : col_pipe_launch<2048, false>(a, m, err, s);
+    case 256: return last ? col_pipe_launch<float, 256, true>(a, m, err, s) : col_pipe_launch<float, 256, false>(a, m, err, s);
+    case 512: return last ? col_pipe_launch<float, 512, true>(a, m, err, s) : col_pipe_launch<float, 512, false>(a, m, err, s);
+    case 1024: return last ? col_pipe_launch<float, 1024, true>(a, m, err, s) : col_pipe_launch<float, 1024, false>(a, m, err, s);
+    case 2048: return last ? col_pipe_launch<float, 2048, true>(a, m, err, s) : col_pipe_launch<float, 2048, false>(a, m, err, s);
   }
   return cudaErrorInvalidValue;
 }
 
-// Tensor map over a batch of FP32 complex planes [nb*nx rows][ny columns],
-// 8-byte elements, box {cols, min(256, nx)} rows; no multicast, no swizzle.
-cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out) {
+// Tensor map over a batch of complex planes [nb*nx rows][ny columns] of
+// 8-byte elements (one per FP32 complex value, two per FP64 one), box
+// {cols, min(256, nx)} rows; no multicast, no swizzle.
+cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out, bool fp64) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult q;
@@ -418,11 +443,12 @@ cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out) 
     if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
-  const int cols = pipe_cols_for(nx);
+  const int cols = pipe_cols_for(nx, fp64);
   if (!cols) return cudaErrorInvalidValue;
-  cuuint64_t dims[2] = {(cuuint64_t)ny, (cuuint64_t)nx * (cuuint64_t)nb};
-  cuuint64_t strides[1] = {(cuuint64_t)ny * 8};
-  cuuint32_t box[2] = {(cuuint32_t)cols, (cuuint32_t)(nx < 256 ? nx : 256)};
+  const int epc = fp64 ? 2 : 1;  // 8-byte elements per complex value
+  cuuint64_t dims[2] = {(cuuint64_t)ny * epc, (cuuint64_t)nx * (cuuint64_t)nb};
+  cuuint64_t strides[1] = {(cuuint64_t)ny * 8 * epc};
+  cuuint32_t box[2] = {(cuuint32_t)(cols * epc), (cuuint32_t)(nx < 256 ? nx : 256)};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = encode(static_cast<CUtensorMap*>(map_out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, psi,
                       dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,

@@ -132,9 +132,9 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
   MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
 
   const bool pipe_col =
-      !fp64 && pipe_supported(g.nx, g.ny) && (ctx->pipe_for(g.nx, g.ny) & MSF_PIPE_COL);
+      pipe_supported(g.nx, g.ny, fp64) && (ctx->pipe_for(g.nx, g.ny) & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
-  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map));
+  if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map, fp64));
   PassArgs row, col;
   row.psi = col.psi = psi.p;
   row.batch_stride = col.batch_stride = plane;
@@ -182,7 +182,7 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
         col.px = pbase + prop_stride * sl;
         col.py = pbase + prop_stride * sl + cbytes * g.nx;
         if (pipe_col)
-          MSF_CUDA(launch_col_slice_pipe(col, sl + 1 == S, col_map, d_err.as<int>(), st));
+          MSF_CUDA(launch_col_slice_pipe(col, sl + 1 == S, col_map, d_err.as<int>(), st, fp64));
         else
           MSF_CUDA(launch_col(fp64, sl + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, st));
       }

@@ -47,7 +47,7 @@ msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
     if ((double)cbytes * plane * b <= 0.5 * (double)free_b) batches.push_back(b);
   if (batches.empty()) batches.push_back(1);
   std::vector<int> pipes{ctx->pipe};
-  if (!ctx->pipe_env && !ctx->fp64 && pipe_supported(g.nx, g.ny)) pipes = {MSF_PIPE_COL, 0};
+  if (!ctx->pipe_env && pipe_supported(g.nx, g.ny, ctx->fp64)) pipes = {MSF_PIPE_COL, 0};
   const int saved_pipe = ctx->pipe;
   ctx->tuned.erase({g.nx, g.ny});  // time_passes then runs ctx->pipe
   msf_context::Tuned best;
