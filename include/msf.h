@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MSF_ABI_VERSION 2
+#define MSF_ABI_VERSION 3
 
 typedef enum {
   MSF_OK = 0,
@@ -157,6 +157,13 @@ typedef struct {
   double* correlograph_probes; /* out: n_x*n_y blocks of n_k*n_phi, raster order */
   double* first_psi;       /* 2*nx*ny: first probe's exit wave in k-space (before
                               any detector MTF)                               */
+  /* out (msf_run): device time of the slice passes of the raster's first
+   * batch, timed with CUDA events on the launching stream while the raster
+   * runs: mean ms of one row pass and of one column pass over the slices
+   * after the first (row) and before the last (column), and the probes that
+   * batch carried; 0 when the raster has fewer than three slices. */
+  double ms_row_pass, ms_col_pass;
+  int32_t pass_batch;
 } msf_results;
 
 /* ---- library ---------------------------------------------------------- */

@@ -1018,12 +1018,24 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   const char* pbase = static_cast<const char*>(spec->prop.p);
   const size_t prop_stride = cbytes * (g.nx + g.ny);
 
+  // events around the passes of the first (eager) batch: the pass times
+  // reported with the results are measured inside the run itself
+  std::vector<cudaEvent_t> pass_ev;
+  bool timing_passes = false;
+  struct EventsGuard {
+    std::vector<cudaEvent_t>* v;
+    ~EventsGuard() {
+      for (cudaEvent_t e : *v) cudaEventDestroy(e);
+    }
+  } pass_ev_guard{&pass_ev};
+
   // one batch: 2*S fused passes then the reductions
   auto enqueue_batch = [&](int nb, const int32_t* shifts_dev, double* amp_out,
                            double* int_out) -> msf_status {
     row.nb = col.nb = nb;
     row.shifts = shifts_dev;
     for (int s = 0; s < S; ++s) {
+      if (timing_passes) MSF_CUDA(cudaEventRecord(pass_ev[3 * s], ctx->stream));
       row.trans = tbase + cbytes * plane * s;
       RowOp op;
       if (fp64) {
@@ -1036,6 +1048,7 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
         MSF_CUDA(launch_row_split_pipe(row, d_err.as<int>(), ctx->stream));
       else
         MSF_CUDA(launch_row(fp64, op, row, ctx->stream));
+      if (timing_passes) MSF_CUDA(cudaEventRecord(pass_ev[3 * s + 1], ctx->stream));
       col.px = pbase + prop_stride * s;
       col.py = pbase + prop_stride * s + cbytes * g.nx;
       if (pipe_col)
@@ -1043,6 +1056,7 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
                                        fp64));
       else
         MSF_CUDA(launch_col(fp64, s + 1 == S ? COL_SLICE_LAST : COL_SLICE, col, ctx->stream));
+      if (timing_passes) MSF_CUDA(cudaEventRecord(pass_ev[3 * s + 2], ctx->stream));
     }
     SplitK sk;
     if (!fp64) {
@@ -1106,8 +1120,15 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
                                sizeof(double) * nb * n_seg, cudaMemcpyDeviceToDevice,
                                ctx->stream));
     } else {
+      timing_passes = p0 == 0 && S >= 3;
+      if (timing_passes) {
+        pass_ev.assign(3 * (size_t)S, nullptr);
+        for (auto& e : pass_ev) MSF_CUDA(cudaEventCreate(&e));
+        res->pass_batch = nb;
+      }
       st = enqueue_batch(nb, P.d_shifts.as<int32_t>() + 2 * p0, P.amp.as<double>() + p0 * n_seg,
                          P.inten.as<double>() + p0 * n_seg);
+      timing_passes = false;
     }
     if (st == MSF_OK && p0 == 0 && res->first_psi) {
       // the first probe's exit wave (adfstem.cpp:2139-2221), before the
@@ -1173,6 +1194,23 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   res->seconds_raster = 1e-3 * ms;
   res->seconds_setup = 0;
   res->probe_slices = n_probes * S;
+  res->ms_row_pass = res->ms_col_pass = 0;
+  if (!pass_ev.empty()) {
+    // row passes of slices 1..S-1 (after the probe-placing first), column
+    // passes of slices 0..S-2 (before the last, which stops in k-space)
+    double row_ms = 0, col_ms = 0;
+    for (int s = 0; s < S; ++s) {
+      float a = 0, b = 0;
+      MSF_CUDA(cudaEventElapsedTime(&a, pass_ev[3 * s], pass_ev[3 * s + 1]));
+      MSF_CUDA(cudaEventElapsedTime(&b, pass_ev[3 * s + 1], pass_ev[3 * s + 2]));
+      if (s >= 1) row_ms += a;
+      if (s + 1 < S) col_ms += b;
+    }
+    res->ms_row_pass = row_ms / (S - 1);
+    res->ms_col_pass = col_ms / (S - 1);
+  } else {
+    res->pass_batch = 0;
+  }
   {
     const int64_t n_batches = (n_probes + B - 1) / B;
     // probe: synth, 2 transform passes, norm, scale (+ FP32 copy); per batch:

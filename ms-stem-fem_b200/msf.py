@@ -18,7 +18,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libmsf.so"
 CLI_PATH = HERE / "bin" / "ms-stem-fem"
-ABI_VERSION = 2  # MSF_ABI_VERSION of the include/msf.h these structs mirror
+ABI_VERSION = 3  # MSF_ABI_VERSION of the include/msf.h these structs mirror
 
 MSF_FP64, MSF_FP32 = 0, 1
 OUT_ADF_IMAGE = 1 << 0
@@ -102,7 +102,9 @@ class Results(C.Structure):
                 ("seconds_raster", C.c_double),
                 ("cap_phi", C.c_int32), ("n_phi", C.c_int32), ("phi_lower", _dp),
                 ("correlograph", _dp), ("correlograph_sqr", _dp),
-                ("correlograph_probes", _dp), ("first_psi", _dp)]
+                ("correlograph_probes", _dp), ("first_psi", _dp),
+                ("ms_row_pass", C.c_double), ("ms_col_pass", C.c_double),
+                ("pass_batch", C.c_int32)]
 
 
 class Request(C.Structure):
@@ -630,6 +632,8 @@ class RunResult:
         self.probe_slices = s.probe_slices
         self.kernel_launches = s.kernel_launches
         self.seconds_raster = s.seconds_raster
+        self.ms_row_pass, self.ms_col_pass = s.ms_row_pass, s.ms_col_pass
+        self.pass_batch = s.pass_batch
         self.adf_image_2d = self.adf_image.reshape(raster.n_x, raster.n_y)
         self.v = {m: self._v[m][:self.n_k] for m in FEM_MODES if detect.outputs & FEM_MODES[m]}
         self.k = self.k_lower[:self.n_k]

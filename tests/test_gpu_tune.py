@@ -60,3 +60,16 @@ def test_cli_writes_and_reuses_wisdom(golden_tmp, tmp_path):
         assert p.returncode == 0, p.stdout + p.stderr
         w = (d / "msf_wisdom_128x128_fp64").read_text()
         assert w.startswith("msf-wisdom 1 ") and " fp64 128 128 " in w
+
+
+def test_run_reports_pass_times_of_its_first_batch():
+    """msf_run times the passes of its first batch with CUDA events: both
+    means are positive and the batch is the context's probes per launch."""
+    j = JobSpec(256, 25.0, 14.0, 400, seed=53, raster_n=6)
+    ctx = msf.Context(precision="fp32", batch=16)
+    spec = ctx.specimen(j.grid, j.pos, j.z)
+    r = ctx.run(spec, j.optics, j.raster, j.detect)
+    assert spec.slices()["n"] >= 3
+    assert r.pass_batch == 16
+    assert r.ms_row_pass > 0 and r.ms_col_pass > 0
+    assert r.ms_row_pass + r.ms_col_pass < 1e3 * r.seconds_raster
