@@ -500,12 +500,17 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    # NCCL over the GPUs by default; MSF_BENCH_DIST_BACKEND=gloo runs the same
+    # sharded flow with the exchange on the host (ranks may then share GPUs)
+    backend = os.environ.get("MSF_BENCH_DIST_BACKEND", "nccl")
+    coll_dev = "cuda" if backend == "nccl" else "cpu"
     if world > 1:
         import datetime
         import torch
         import torch.distributed as dist
+        local = local % max(1, torch.cuda.device_count())
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
 
     work = Path(tempfile.mkdtemp(prefix="msf_bench_r%d_" % rank))
     spec_path = work / "c2.data"
@@ -546,13 +551,25 @@ def main():
                               yp_w.ctypes.data_as(msf._dp))
 
         def step():
+            # device time of this rank's probes (msf's own events on its
+            # stream) + device time of the exchange (events on the stream the
+            # collectives run on; host clock with gloo) + the host finish
+            part = shards.run_shard(ctx, spec, job.optics, raster_w, job.detect, rank, world)
+            t_x = time.perf_counter()
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record()
-            res, part = shards.run_sharded(ctx, spec, job.optics, raster_w, job.detect, rank,
-                                           world, dist, device="cuda")
+            amp, inten, acc_a, acc_i = shards.exchange(part, raster_w.n_x * raster_w.n_y, world,
+                                                       dist, coll_dev,
+                                                       job.grid.nx * job.grid.ny)
             ev1.record()
             torch.cuda.synchronize()
-            return res, part, 1e-3 * ev0.elapsed_time(ev1)
+            t_x = (1e-3 * ev0.elapsed_time(ev1) if coll_dev == "cuda"
+                   else time.perf_counter() - t_x)
+            t_f = time.perf_counter()
+            res = msf.finish(spec.grid, job.optics, raster_w, job.detect, amp, inten, acc_a,
+                             acc_i)
+            t_f = time.perf_counter() - t_f
+            return res, part, part["seconds_raster"] + t_x + t_f
     for _ in range(args.warmup):
         if world > 1:
             step()
@@ -580,7 +597,7 @@ def main():
     total_dev = sum(dev_times)
     if dist is not None:
         import torch
-        t = torch.tensor([total_dev], device="cuda")
+        t = torch.tensor([total_dev], device=coll_dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_dev = float(t.item())
     value = ps * world / total_dev  # ps: this rank's probe*slices (equal shards)
@@ -631,7 +648,7 @@ def main():
             s2 = ctx.specimen(job.grid, q, z)
             if world > 1:
                 _, p2 = shards.run_sharded(ctx, s2, job.optics, raster_w, job.detect, rank,
-                                           world, dist, device="cuda")
+                                           world, dist, device=coll_dev)
                 e2e_ps += p2["probe_slices"]
             else:
                 r2 = ctx.run(s2, job.optics, job.raster, job.detect)
@@ -646,7 +663,7 @@ def main():
                "includes": "atom upload, LUT/slicing/transmission build, raster, result copy"}
         if dist is not None:
             import torch
-            t = torch.tensor([e2e_t], device="cuda")
+            t = torch.tensor([e2e_t], device=coll_dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e["value"] = e2e_ps * world / float(t.item())
 
