@@ -184,7 +184,7 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
 #ifndef MSF_COL_PIPE_THREADS_PER_SM
 #define MSF_COL_PIPE_THREADS_PER_SM 256
 #endif
-constexpr int ctas_per_256(int threads) {
+constexpr int col_pipe_min_ctas(int threads) {
   return threads >= MSF_COL_PIPE_THREADS_PER_SM ? 1 : MSF_COL_PIPE_THREADS_PER_SM / threads;
 }
 
@@ -194,7 +194,7 @@ constexpr int ctas_per_256(int threads) {
 // LAST is then taken per probe from its slot.
 template <typename Real, int N, int COLS, bool LAST, bool SLOTS>
 __global__ void __launch_bounds__(COLS * Shape<N, Real>::T,
-                                  ctas_per_256(COLS * Shape<N, Real>::T))
+                                  col_pipe_min_ctas(COLS * Shape<N, Real>::T))
 col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap, int* err) {
   using C = Cx<Real>;
   using Sh = Shape<N, Real>;
