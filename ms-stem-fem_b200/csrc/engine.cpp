@@ -346,6 +346,29 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
   }
   MSF_TRY(upload(ctx, &spec->mask_lo, lo));
   MSF_TRY(upload(ctx, &spec->mask_hi, hi));
+  {
+    // a column keeps no kx at all when lo = 0 and hi = nx
+    std::vector<uint8_t> dead(g.ny);
+    for (int j = 0; j < g.ny; ++j) dead[j] = lo[j] == 0 && hi[j] == g.nx;
+    spec->n_live_columns = (int)std::count(dead.begin(), dead.end(), 0);
+    const bool fp = ctx->fp64;
+    const int T = row_line_threads(g.ny, fp), cols = pipe_cols_for(g.nx, fp);
+    if (T > 0 && g.ny / T <= 32 && cols > 0 && spec->n_live_columns < g.ny) {
+      std::vector<uint32_t> bits(T, 0u);
+      for (int t = 0; t < T; ++t)
+        for (int m = 0; m < g.ny / T; ++m)
+          if (dead[t + T * m]) bits[t] |= 1u << m;
+      std::vector<int32_t> groups;
+      for (int gi = 0; gi < g.ny / cols; ++gi) {
+        bool live = false;
+        for (int c = 0; c < cols; ++c) live = live || !dead[gi * cols + c];
+        if (live) groups.push_back(gi);
+      }
+      MSF_TRY(upload(ctx, &spec->dead_bits, bits));
+      MSF_TRY(upload(ctx, &spec->live_groups, groups));
+      spec->n_live_groups = (int)groups.size();
+    }
+  }
 
   // transmission functions (slice.cpp:1544-1757)
   const size_t cbytes = ctx->fp64 ? 16 : 8;
@@ -486,6 +509,11 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   MSF_TRY(ctx->alloc(&d_err, sizeof(int)));
   MSF_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
   if (pipe_col) MSF_CUDA(encode_column_map(psi.p, nb, g.nx, g.ny, col_map, fp64));
+  if (pipe_col && !pipe_row && spec->n_live_groups > 0) {  // skip removed columns
+    row.row_dead_bits = spec->dead_bits.as<uint32_t>();
+    col.live_groups = spec->live_groups.as<int32_t>();
+    col.n_live_groups = spec->n_live_groups;
+  }
   auto row_pass = [&]() {
     return pipe_row ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
                     : launch_row(fp64, rop, row, ctx->stream);
@@ -1003,6 +1031,11 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map, fp64));
 
   PassArgs row, col;
+  if (pipe_col && !pipe_row && spec->n_live_groups > 0) {  // skip removed columns
+    row.row_dead_bits = spec->dead_bits.as<uint32_t>();
+    col.live_groups = spec->live_groups.as<int32_t>();
+    col.n_live_groups = spec->n_live_groups;
+  }
   row.psi = col.psi = psi.p;
   row.batch_stride = col.batch_stride = plane;
   row.nx = col.nx = g.nx;

@@ -115,6 +115,10 @@ struct msf_specimen {
   msf::DevBuf t;              // [slice][nx][ny] complex, context precision
   msf::DevBuf prop;           // [slice] {px[nx], py[ny]} complex, context precision
   msf::DevBuf mask_lo, mask_hi;
+  // columns the band limit removes entirely: row-pass zero bits, and the
+  // column groups of the pipelined column pass that keep any column
+  msf::DevBuf dead_bits, live_groups;
+  int n_live_groups = 0, n_live_columns = 0;
   msf::DevBuf kx, ky;         // FP64 domains for device set-up kernels
   std::vector<double> hprop;  // FP64 propagators, host copy
   double seconds_setup = 0;

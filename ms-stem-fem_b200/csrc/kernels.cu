@@ -210,6 +210,15 @@ row_kernel(const PassArgs a) {
     }
     fft_line<Sh, false>(v, sm, t, tw, sync);
   }
+  if constexpr (OP == ROW_SLICE || OP == ROW_SLICE_FIRST || OP == ROW_SPLIT ||
+                OP == ROW_SPLIT_FIRST) {
+    if (a.row_dead_bits) {  // columns the next band limit removes entirely
+      const uint32_t dead = __ldg(a.row_dead_bits + t);
+#pragma unroll
+      for (int m = 0; m < E; ++m)
+        if ((dead >> m) & 1u) v[m] = C{(Real)0, (Real)0};
+    }
+  }
 #pragma unroll
   for (int m = 0; m < E; ++m) row[t + T * m] = v[m];
 }
@@ -863,6 +872,19 @@ inline unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1)
 
 bool supported_length(int n) {
   return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096;
+}
+
+int row_line_threads(int n, bool fp64) {
+  switch (n) {
+    case 64: return fp64 ? Shape<64, double>::T : Shape<64, float>::T;
+    case 128: return fp64 ? Shape<128, double>::T : Shape<128, float>::T;
+    case 256: return fp64 ? Shape<256, double>::T : Shape<256, float>::T;
+    case 512: return fp64 ? Shape<512, double>::T : Shape<512, float>::T;
+    case 1024: return fp64 ? Shape<1024, double>::T : Shape<1024, float>::T;
+    case 2048: return fp64 ? Shape<2048, double>::T : Shape<2048, float>::T;
+    case 4096: return fp64 ? Shape<4096, double>::T : Shape<4096, float>::T;
+  }
+  return 0;
 }
 
 cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s) {

@@ -75,6 +75,14 @@ struct PassArgs {
   const void* psi0 = nullptr;
   // slot batches (ROW_SLOTS, COL_SLOTS, pipelined column pass): [nb]
   const SlotPass* slots = nullptr;
+  // Columns the band limit removes entirely (lo = 0, hi = nx: no kx kept):
+  // the slice row passes store zeros there (bit m of word t: column
+  // t + T*m, T the row transform's threads per line) ...
+  const uint32_t* row_dead_bits = nullptr;
+  // ... so the pipelined column pass skips the column groups that hold only
+  // such columns: it walks live_groups[n_live_groups] (nullptr: all groups)
+  const int32_t* live_groups = nullptr;
+  int n_live_groups = 0;
 };
 
 // Vacuum part of the exit wave for split-wave detection: k-space values of
@@ -89,6 +97,10 @@ struct SplitK {
 
 // Returns false if the length is not supported.
 bool supported_length(int n);
+// Threads per line of the row transform of length n (its T); 0 if unsupported.
+int row_line_threads(int n, bool fp64);
+// Columns per tile of the pipelined column pass (0 if unsupported).
+int pipe_cols_for(int nx, bool fp64);
 cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s);
 cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s);
 

@@ -209,10 +209,15 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
   __shared__ uint64_t bars[2];
   __shared__ int flag;
   const int c = threadIdx.x % COLS, t = threadIdx.x / COLS;
-  const int items = a.nb * (a.ny / COLS);
+  // column groups to walk: all, or those with any column the band limit
+  // keeps (the row pass stored zeros in the others)
+  const int groups = a.live_groups ? a.n_live_groups : a.ny / COLS;
+  const int items = a.nb * groups;
+  auto group_of = [&](int gi) { return a.live_groups ? __ldg(a.live_groups + gi) : gi; };
   auto sync = [] { __syncthreads(); };
   auto issue = [&](int item, int which) {
-    const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
+    const int gi = item / a.nb, b = item - gi * a.nb;
+    const int g = group_of(gi);
     C* dst = bufs + which * BUF;
     mbar_expect_tx(&bars[which], N * COLS * (int)sizeof(C));
 #pragma unroll
@@ -245,7 +250,8 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
       return;
     }
     parity[w] ^= 1;
-    const int g = item / a.nb, b = item - (item / a.nb) * a.nb;
+    const int gi = item / a.nb, b = item - gi * a.nb;
+    const int g = group_of(gi);
     const int j = g * COLS + c;
     const int32_t* mask_lo = a.mask_lo;
     const int32_t* mask_hi = a.mask_hi;
@@ -357,7 +363,8 @@ cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
   }
-  const int items = a.nb * (a.ny / CC);
+  const int items = a.nb * (a.live_groups ? a.n_live_groups : a.ny / CC);
+  if (items <= 0) return cudaSuccess;
   const int grid = items < per_sm * sm_count() ? items : per_sm * sm_count();
   k<<<grid, CC * Shape<N, Real>::T, smem, s>>>(a, map, err);
   return cudaGetLastError();

@@ -136,6 +136,9 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
   alignas(64) unsigned char col_map[128];
   if (pipe_col) MSF_CUDA(encode_column_map(psi.p, B, g.nx, g.ny, col_map, fp64));
   PassArgs row, col;
+  // columns the band limit removes entirely are skipped (same grid, hence
+  // the same mask, for every snapshot)
+  const bool skip_dead = pipe_col && snaps[0]->n_live_groups > 0;
   row.psi = col.psi = psi.p;
   row.batch_stride = col.batch_stride = plane;
   row.nx = col.nx = g.nx;
@@ -166,6 +169,11 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
       row.probe = P.probe64.p;
       col.mask_lo = spec->mask_lo.as<int32_t>();
       col.mask_hi = spec->mask_hi.as<int32_t>();
+      if (skip_dead) {
+        row.row_dead_bits = spec->dead_bits.as<uint32_t>();
+        col.live_groups = spec->live_groups.as<int32_t>();
+        col.n_live_groups = spec->n_live_groups;
+      }
       const char* tbase = static_cast<const char*>(spec->t.p);
       const char* pbase = static_cast<const char*>(spec->prop.p);
       const size_t prop_stride = cbytes * (g.nx + g.ny);
