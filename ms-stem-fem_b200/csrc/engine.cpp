@@ -511,6 +511,7 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   if (pipe_col) MSF_CUDA(encode_column_map(psi.p, nb, g.nx, g.ny, col_map, fp64));
   if (pipe_col && !pipe_row && spec->n_live_groups > 0) {  // skip removed columns
     row.row_dead_bits = spec->dead_bits.as<uint32_t>();
+    row.row_dead_io = 3;  // a slice between the first and the last
     col.live_groups = spec->live_groups.as<int32_t>();
     col.n_live_groups = spec->n_live_groups;
   }
@@ -1068,6 +1069,9 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
     row.nb = col.nb = nb;
     row.shifts = shifts_dev;
     for (int s = 0; s < S; ++s) {
+      // removed columns: not read after the first slice, not stored before
+      // the last (which leaves zeros there for the detection)
+      row.row_dead_io = (s > 0 ? 1 : 0) | (s + 1 < S ? 2 : 0);
       if (timing_passes) MSF_CUDA(cudaEventRecord(pass_ev[3 * s], ctx->stream));
       row.trans = tbase + cbytes * plane * s;
       RowOp op;

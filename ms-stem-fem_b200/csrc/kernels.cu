@@ -178,6 +178,13 @@ row_kernel(const PassArgs a) {
   } else if constexpr (OP == ROW_SPLIT_FIRST) {
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
+  } else if constexpr (OP == ROW_SPLIT || OP == ROW_SLICE) {
+    // columns removed by the band limit were not stored: they are zero
+    const uint32_t skip = (a.row_dead_bits && (a.row_dead_io & 1)) ? __ldg(a.row_dead_bits + t)
+                                                                  : 0u;
+#pragma unroll
+    for (int m = 0; m < E; ++m)
+      v[m] = ((skip >> m) & 1u) ? C{(Real)0, (Real)0} : row[t + T * m];
   } else {
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = row[t + T * m];
@@ -214,6 +221,12 @@ row_kernel(const PassArgs a) {
                 OP == ROW_SPLIT_FIRST) {
     if (a.row_dead_bits) {  // columns the next band limit removes entirely
       const uint32_t dead = __ldg(a.row_dead_bits + t);
+      if (a.row_dead_io & 2) {  // nobody reads them: leave them unstored
+#pragma unroll
+        for (int m = 0; m < E; ++m)
+          if (!((dead >> m) & 1u)) row[t + T * m] = v[m];
+        return;
+      }
 #pragma unroll
       for (int m = 0; m < E; ++m)
         if ((dead >> m) & 1u) v[m] = C{(Real)0, (Real)0};

@@ -79,6 +79,10 @@ struct PassArgs {
   // the slice row passes store zeros there (bit m of word t: column
   // t + T*m, T the row transform's threads per line) ...
   const uint32_t* row_dead_bits = nullptr;
+  // with row_dead_bits: bit 0, this pass's input was not stored in those
+  // columns (read them as zero); bit 1, its output there need not be stored
+  // (the next pass reads none of it)
+  int row_dead_io = 0;
   // ... so the pipelined column pass skips the column groups that hold only
   // such columns: it walks live_groups[n_live_groups] (nullptr: all groups)
   const int32_t* live_groups = nullptr;

@@ -179,6 +179,7 @@ msf_status run_md(msf_context* ctx, int n_snap, const msf_specimen* const* snaps
       const size_t prop_stride = cbytes * (g.nx + g.ny);
       for (int sl = 0; sl < S; ++sl) {
         row.trans = tbase + cbytes * plane * sl;
+        row.row_dead_io = (sl > 0 ? 1 : 0) | (sl + 1 < S ? 2 : 0);
         RowOp op;
         if (fp64) {
           op = sl == 0 ? ROW_SLICE_FIRST : ROW_SLICE;
