@@ -622,7 +622,10 @@ def main():
         timing = "msf_time_passes after the timed region"
     n = job.grid.nx
     cbytes = 8 if args.precision == "fp32" else 16
-    alg = 2.0 * n * n * cbytes * nb  # read + write of nb wavefields per pass
+    # read + write of nb wavefields per pass, less the columns the band limit
+    # removes entirely (zero between the passes: neither pass moves them)
+    live = spec.live_columns() / float(job.grid.ny)
+    alg = 2.0 * n * n * cbytes * nb * live
     dom = "col" if ms_col >= ms_row else "row"
     t_dom = max(ms_row, ms_col) * 1e-3
     peak, peak_kind = measured_peaks()
@@ -635,7 +638,8 @@ def main():
                 "kernel": "%s pass (fused FFT + %s), %d probes/launch" %
                           (dom, "transmission" if dom == "row" else "propagator", nb),
                 "peak_source": peak_kind, "ms_row": round(ms_row, 4), "ms_col": round(ms_col, 4),
-                "algorithmic_bytes_per_launch": alg, "timing": timing}
+                "algorithmic_bytes_per_launch": alg, "live_column_fraction": round(live, 4),
+                "timing": timing}
 
     # end to end through the C ABI from host buffers
     e2e = None

@@ -195,6 +195,10 @@ msf_status msf_specimen_transmission(const msf_specimen* spec, int32_t slice,
                                      double* out);
 /* Bytes of device memory the specimen holds. */
 int64_t msf_specimen_device_bytes(const msf_specimen* spec);
+/* Columns (ky values) in which the band limit keeps any kx (bw_limit.cpp:
+ * 30-47 with the transmission cut-off); the slice passes move no data for
+ * the others, which only ever hold zeros between the passes. */
+int32_t msf_specimen_live_columns(const msf_specimen* spec);
 
 /* ---- the multislice raster (adfstem) ----------------------------------- */
 msf_status msf_run(msf_context* ctx, const msf_specimen* spec,

@@ -194,6 +194,10 @@ int64_t msf_specimen_device_bytes(const msf_specimen* spec) {
   return spec ? spec->device_bytes : 0;
 }
 
+int32_t msf_specimen_live_columns(const msf_specimen* spec) {
+  return spec ? spec->n_live_columns : 0;
+}
+
 msf_status msf_run(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                    const msf_raster* raster, const msf_detect* detect, msf_results* results) {
   if (!ctx || !spec || spec->ctx != ctx) {

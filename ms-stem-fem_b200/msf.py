@@ -46,6 +46,7 @@ EXPORTED = [
     "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
     "msf_finish", "msf_run_plain", "msf_amorphous_positions", "msf_run_md", "msf_md_main",
     "msf_tune", "msf_wisdom_export", "msf_wisdom_import", "msf_server_cancel",
+    "msf_specimen_live_columns",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -149,6 +150,8 @@ def lib() -> C.CDLL:
         L.msf_specimen_transmission.argtypes = [C.c_void_p, C.c_int32, _dp]
         L.msf_specimen_device_bytes.argtypes = [C.c_void_p]
         L.msf_specimen_device_bytes.restype = C.c_int64
+        L.msf_specimen_live_columns.argtypes = [C.c_void_p]
+        L.msf_specimen_live_columns.restype = C.c_int32
         L.msf_run.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics), C.POINTER(Raster),
                               C.POINTER(Detect), C.POINTER(Results)]
         L.msf_probe.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics), _dp]
@@ -571,6 +574,10 @@ class Specimen:
 
     def device_bytes(self) -> int:
         return lib().msf_specimen_device_bytes(self._h)
+
+    def live_columns(self) -> int:
+        """Columns in which the band limit keeps any kx."""
+        return lib().msf_specimen_live_columns(self._h)
 
 
 class RunResult:
