@@ -367,6 +367,8 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
       MSF_TRY(upload(ctx, &spec->dead_bits, bits));
       MSF_TRY(upload(ctx, &spec->live_groups, groups));
       spec->n_live_groups = (int)groups.size();
+      spec->h_dead_bits = bits;
+      spec->h_live_groups = groups;
     }
   }
 

@@ -118,6 +118,8 @@ struct msf_specimen {
   // columns the band limit removes entirely: row-pass zero bits, and the
   // column groups of the pipelined column pass that keep any column
   msf::DevBuf dead_bits, live_groups;
+  std::vector<uint32_t> h_dead_bits;  // host copies (slot lanes compare them)
+  std::vector<int32_t> h_live_groups;
   int n_live_groups = 0, n_live_columns = 0;
   msf::DevBuf kx, ky;         // FP64 domains for device set-up kernels
   std::vector<double> hprop;  // FP64 propagators, host copy

@@ -149,19 +149,28 @@ row_kernel(const PassArgs a) {
     // slot batch: this CTA's probe reads its own slice tables
     const SlotPass sp = a.slots[b];
     if (sp.op == SLOT_IDLE) return;
+    // columns the band limit removes entirely (when the lane skips them):
+    // never loaded, stored (as zeros) only at the slot's last slice
+    const uint32_t dead = a.row_dead_bits ? __ldg(a.row_dead_bits + t) : 0u;
     if (sp.op == SLOT_FIRST) {
 #pragma unroll
       for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
     } else {
 #pragma unroll
-      for (int m = 0; m < E; ++m) v[m] = row[t + T * m];
+      for (int m = 0; m < E; ++m)
+        v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : row[t + T * m];
       fft_line<Sh, true>(v, sm, t, tw, sync);
     }
     split_update<Sh>(v, static_cast<const C*>(sp.psi0), static_cast<const C*>(sp.trans), a.nx,
                      i, t, sp.sx, sp.sy, (Real)a.inv_s);
     fft_line<Sh, false>(v, sm, t, tw, sync);
 #pragma unroll
-    for (int m = 0; m < E; ++m) row[t + T * m] = v[m];
+    for (int m = 0; m < E; ++m) {
+      if (!((dead >> m) & 1u))
+        row[t + T * m] = v[m];
+      else if (sp.last)
+        row[t + T * m] = C{(Real)0, (Real)0};
+    }
     return;
   }
   if constexpr (OP == ROW_SLICE_FIRST) {

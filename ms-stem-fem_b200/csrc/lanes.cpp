@@ -105,6 +105,50 @@ msf_status Lane::add(SlotJob* job) {
   }
   if (job->plan.n_chunks > max_chunks_) MSF_TRY(grow_chunks(job->plan.n_chunks));
   row_.inv_s = col_.inv_s = 1.0 / g.s;
+  const msf_specimen* spec = job->plan.spec;
+  if (!skip_decided_) {
+    skip_decided_ = true;
+    if (pipe_col_ && spec->n_live_groups > 0) {
+      MSF_TRY(ctx_->alloc(&dead_bits_, spec->dead_bits.bytes));
+      MSF_TRY(ctx_->alloc(&live_groups_, spec->live_groups.bytes));
+      MSF_CUDA(cudaMemcpyAsync(dead_bits_.p, spec->dead_bits.p, spec->dead_bits.bytes,
+                               cudaMemcpyDeviceToDevice, stream_));
+      MSF_CUDA(cudaMemcpyAsync(live_groups_.p, spec->live_groups.p, spec->live_groups.bytes,
+                               cudaMemcpyDeviceToDevice, stream_));
+      h_live_ = spec->h_live_groups;
+      h_dead_cols_.assign(ny_, 0);
+      const int T = row_line_threads(ny_, false);
+      for (int t = 0; t < T; ++t)
+        for (int m = 0; m < ny_ / T; ++m)
+          if ((spec->h_dead_bits[t] >> m) & 1u) h_dead_cols_[t + T * m] = 1;
+      row_.row_dead_bits = dead_bits_.as<uint32_t>();
+      col_.live_groups = live_groups_.as<int32_t>();
+      col_.n_live_groups = (int)h_live_.size();
+      skip_ = true;
+    }
+  } else if (skip_ && (spec->n_live_groups == 0 || spec->h_live_groups != h_live_)) {
+    // a raster whose band limit removes other columns: every pass from now
+    // on moves all columns.  The slots in flight hold stale values in the
+    // columns that were skipped, which are zero in the full computation:
+    // write those zeros first.
+    MSF_CUDA(cudaStreamSynchronize(stream_));
+    if (graph_pass_) {
+      cudaGraphExecDestroy(graph_pass_);
+      graph_pass_ = nullptr;
+    }
+    for (int j0 = 0; j0 < ny_;) {
+      if (!h_dead_cols_[j0]) { ++j0; continue; }
+      int j1 = j0;
+      while (j1 < ny_ && h_dead_cols_[j1]) ++j1;
+      MSF_CUDA(cudaMemset2DAsync(static_cast<char*>(psi_.p) + 8 * (size_t)j0, 8 * (size_t)ny_,
+                                 0, 8 * (size_t)(j1 - j0), (size_t)nx_ * B_, stream_));
+      j0 = j1;
+    }
+    row_.row_dead_bits = nullptr;
+    col_.live_groups = nullptr;
+    col_.n_live_groups = 0;
+    skip_ = false;
+  }
   job->next_probe = 0;
   job->started = job->done = 0;
   job->complete = false;

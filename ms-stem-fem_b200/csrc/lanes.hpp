@@ -84,6 +84,12 @@ class Lane {
   DevBuf psi_, table_, partial_, err_;
   int max_chunks_ = 0;
   bool pipe_col_ = false;
+  // removed-column skipping: on while every raster the lane was given has
+  // the same removed columns (the first one's); off for good otherwise
+  bool skip_ = false, skip_decided_ = false;
+  std::vector<int32_t> h_live_;
+  std::vector<uint8_t> h_dead_cols_;  // [ny] 1: removed while skipping
+  DevBuf dead_bits_, live_groups_;
   alignas(64) unsigned char col_map_[128];
   PassArgs row_, col_;
   size_t table_bytes_ = 0;

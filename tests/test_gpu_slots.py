@@ -169,3 +169,32 @@ def test_server_cancel():
     st = srv.stats()
     assert st["completed"] == 1 and st["failed"] == 2
     srv.close()
+
+
+def rect_job(seed=62):
+    """256^2 grid over a 25 x 20 A cell: its band limit removes other
+    columns than a square cell's."""
+    j = JobSpec(256, 25.0, 14.0, 300, seed=seed, raster_n=6)
+    j.pos = specimen.amorphous_positions(240, (25.0, 20.0, 14.0), seed=seed)
+    j.z = np.full(len(j.pos), 14, dtype=np.uint32)
+    j.grid = msf.Grid(nx=256, ny=256, voltage=200000.0, xperiod=25.0, yperiod=20.0,
+                      zperiod=14.0, dupe_x=1, dupe_y=1, dupe_z=1, replicate_atoms=0,
+                      xmin=0.0, ymin=0.0, zmin=0.0, min_slice=2.0)
+    j.yp = np.arange(6) * (20.0 / 6)
+    j.raster = msf.Raster(6, 6, j.xp.ctypes.data_as(msf._dp), j.yp.ctypes.data_as(msf._dp))
+    return j
+
+
+def test_lane_stops_skipping_removed_columns_midflight():
+    """A lane skips the columns its first raster's band limit removes; a
+    raster of the same grid size with other removed columns makes it move
+    every column from then on, zeroing the skipped ones in the slots in
+    flight.  Both rasters give exactly what they give alone."""
+    a = JobSpec(256, 25.0, 40.0, 1000, seed=63, raster_n=24)
+    b = rect_job()
+    alone = [serve([j], slots=4)[0][0] for j in (a, b)]
+    mixed, _ = serve([a, b], slots=4, stagger_s=0.05)
+    for k, (m, r) in enumerate(zip(mixed, alone)):
+        assert np.array_equal(m.adf_image, r.adf_image), k
+        for mode in r.v:
+            assert np.array_equal(m.v[mode], r.v[mode], equal_nan=True), (k, mode)
