@@ -146,30 +146,37 @@ row_kernel(const PassArgs a) {
   };
   C v[E];
   if constexpr (OP == ROW_SLOTS) {
-    // slot batch: this CTA's probe reads its own slice tables
+    // slot batch: this CTA's probe reads its own slice tables.  The row
+    // loads wait for the slot entry, so a CTA takes nx / (LINES * gridDim.y)
+    // consecutive row groups of its slot and pays that wait once.
     const SlotPass sp = a.slots[b];
     if (sp.op == SLOT_IDLE) return;
     // columns the band limit removes entirely (when the lane skips them):
     // never loaded, stored (as zeros) only at the slot's last slice
     const uint32_t dead = a.row_dead_bits ? __ldg(a.row_dead_bits + t) : 0u;
-    if (sp.op == SLOT_FIRST) {
+    const int groups = a.nx / (LINES * (int)gridDim.y);
+    for (int r = 0; r < groups; ++r) {
+      const int ir = ((int)blockIdx.y * groups + r) * LINES + line;
+      C* rrow = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)ir * N;
+      if (sp.op == SLOT_FIRST) {
 #pragma unroll
-      for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
-    } else {
+        for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
+      } else {
 #pragma unroll
-      for (int m = 0; m < E; ++m)
-        v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : row[t + T * m];
-      fft_line<Sh, true>(v, sm, t, tw, sync);
-    }
-    split_update<Sh>(v, static_cast<const C*>(sp.psi0), static_cast<const C*>(sp.trans), a.nx,
-                     i, t, sp.sx, sp.sy, (Real)a.inv_s);
-    fft_line<Sh, false>(v, sm, t, tw, sync);
+        for (int m = 0; m < E; ++m)
+          v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : rrow[t + T * m];
+        fft_line<Sh, true>(v, sm, t, tw, sync);
+      }
+      split_update<Sh>(v, static_cast<const C*>(sp.psi0), static_cast<const C*>(sp.trans),
+                       a.nx, ir, t, sp.sx, sp.sy, (Real)a.inv_s);
+      fft_line<Sh, false>(v, sm, t, tw, sync);
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-      if (!((dead >> m) & 1u))
-        row[t + T * m] = v[m];
-      else if (sp.last)
-        row[t + T * m] = C{(Real)0, (Real)0};
+      for (int m = 0; m < E; ++m) {
+        if (!((dead >> m) & 1u))
+          rrow[t + T * m] = v[m];
+        else if (sp.last)
+          rrow[t + T * m] = C{(Real)0, (Real)0};
+      }
     }
     return;
   }
@@ -337,7 +344,14 @@ cudaError_t row_launch(const PassArgs& a, cudaStream_t s) {
     configured = true;
   }
   if (a.nx % L != 0) return cudaErrorInvalidValue;
-  dim3 grid(a.nb, a.nx / L);
+  int groups = a.nx / L;
+  if constexpr (OP == ROW_SLOTS) {
+    // up to 4 row groups per CTA while a slot keeps 256 CTAs
+    int per = 1;
+    while (per < 4 && groups % (2 * per) == 0 && groups / (2 * per) >= 256) per *= 2;
+    groups /= per;
+  }
+  dim3 grid(a.nb, groups);
   k<<<grid, L * Sh::T, smem, s>>>(a);
   return cudaGetLastError();
 }

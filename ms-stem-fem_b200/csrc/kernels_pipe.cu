@@ -242,6 +242,10 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
   int k = 0;
   for (; item < items; ++k, item += gridDim.x) {
     const int w = k & 1;
+    // a slot batch reads its slot entry before the tile wait, so that the
+    // load overlaps the copy instead of following it
+    SlotPass sp{};
+    if constexpr (SLOTS) sp = a.slots[item % a.nb];
     if (!cta_wait(&bars[w], parity[w], &flag)) {
       if (threadIdx.x == 0) {
         atomicExch(err, 1);
@@ -259,7 +263,6 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
     const C* pyb = static_cast<const C*>(a.py);
     bool idle = false, stop_in_k = LAST;
     if constexpr (SLOTS) {
-      const SlotPass& sp = a.slots[b];  // uniform over the CTA
       idle = sp.op == SLOT_IDLE;
       mask_lo = sp.mask_lo;
       mask_hi = sp.mask_hi;
