@@ -1,5 +1,5 @@
 """CUDA path against the reference's own results (golden fixtures) and the
-CPU oracle.  Tolerances (BASELINE north star): ADF image and V(k) within
+CPU oracle.  Tolerances: ADF image and V(k) within
 1e-5 relative on the FP64 path and 1e-4 on the FP32 path; slicing, pixel
 snaps and bins bit-exact.  V(k) also gets an absolute floor for bins where
 V itself is at the cancellation floor of n*sum(A^2)/sum(A)^2 - 1."""
