@@ -510,7 +510,10 @@ def main():
         import torch.distributed as dist
         local = local % max(1, torch.cuda.device_count())
         torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        # every rank runs the same collectives at most one raster step
+        # (seconds) apart: a rank that stops ends the others' next
+        # collective with an error within this bound instead of a hang
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
 
     work = Path(tempfile.mkdtemp(prefix="msf_bench_r%d_" % rank))
     spec_path = work / "c2.data"
