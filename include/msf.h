@@ -216,15 +216,20 @@ msf_status msf_run_plain(msf_context* ctx, const msf_specimen* spec,
 msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
                      const msf_optics* optics, double* out);
 
-/* The probe of msf_probe written into caller-provided device memory
+/* The probe of msf_probe, to within FP64 rounding (1e-12 of its largest
+ * value; the twiddles come from the device's sincospi rather than host
+ * cos/sin, so not bit for bit), written into caller-provided device memory
  * (2*nx*ny doubles) on `stream` (a cudaStream_t, NULL for the default
  * stream), allocating no device memory.  No counterpart in the reference.
  * For callers that may not call cudaMalloc (an application that owns all
  * device memory in its own pool, a running loop that must not stall on an
  * allocation).  Its scratch is one fixed device array per device, sized for
- * grids of at most 2048 x 2048; larger grids return MSF_ERR_ARG.  The first
- * call on a device looks up that array's address and should come before any
- * stream capture; calls that overlap on the GPU share the array and race. */
+ * grids of at most 2048 x 2048; larger grids return MSF_ERR_ARG.  A call
+ * that is not being captured looks up that array's address (again on every
+ * such call, so a device reset leaves nothing stale); a captured call uses
+ * the address of the last uncaptured call on its device, so one uncaptured
+ * call must come first.  Calls that overlap on the GPU share the array and
+ * race. */
 msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
                              double* probe_device, void* stream);
 
@@ -233,13 +238,18 @@ msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
 typedef struct {
   int32_t nx, ny;             /* grid                                          */
   int32_t batch;              /* probes per launch chosen                      */
-  int32_t pipe;               /* pipelined FP32 passes: bit 0 column, bit 1 row */
+  int32_t pipe;               /* slice-pass variants: bit 0 pipelined column
+                                 pass, bit 1 pipelined row pass, bit 2 row
+                                 pass with staged slice tables (FP32), bit 3
+                                 that row pass's alternative FFT radix
+                                 schedule                                    */
   double ns_per_probe_slice;  /* measured time of the two slice passes        */
 } msf_tuning;
 /* Times the two slice passes of `spec`'s grid (CUDA events, after a
  * warm-up) for each candidate probes-per-launch (8 .. 256, within half the
- * free memory) and, for FP32 grids the pipelined passes support, with and
- * without the pipelined column pass; records the fastest per probe*slice
+ * free memory) and each slice-pass variant the grid supports (pipelined
+ * column pass or not; for FP32, staged row pass or not, in either FFT radix
+ * schedule); records the fastest per probe*slice
  * in the context, where msf_run / msf_run_md / msf_run_partial use it for
  * that grid unless the context's batch or MSF_PIPE fixes the choice. */
 msf_status msf_tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out);

@@ -65,7 +65,9 @@ def mass_rules(src: Path) -> str:
 
 
 def main() -> None:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_tables.py <path of the reference ms-stem-fem checkout>")
+    ref = Path(sys.argv[1])
     src = ref / "src"
     here = Path(__file__).resolve().parent
     (here / "kirkland_table.inc").write_text(kirkland(src))

@@ -10,9 +10,14 @@
 // device array, sized for grids of at most kMaxSide x kMaxSide.
 //
 // Behaviour a caller must know:
-//  * The first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture on the device.
+//  * A call that is not being captured looks up the array's device address
+//    (cudaGetSymbolAddress) with its device current, every time; a call
+//    inside a stream capture uses the address of the last uncaptured call
+//    on that device, so make one call before any capture (and again after
+//    a cudaDeviceReset, before capturing).
+//  * The probe equals msf_probe's to within FP64 rounding (1e-12 of its
+//    largest value), not bit for bit: the twiddles here come from the
+//    device's sincospi, msf_probe's from host cos/sin.
 //  * Every call on a device shares the one array and leaves its contents
 //    behind.  Each call overwrites every scratch entry it reads, so nothing
 //    has to start at zero, but two calls whose work overlaps on the GPU (for
@@ -47,10 +52,20 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 void* g_address[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device, looked up once.
-msf_status scratch_address(int device, unsigned char** out) {
+// Device address of the scratch array on the current device.  Outside a
+// stream capture it is looked up again on every call (a host-side query
+// that allocates nothing), so a context the application tore down and
+// recreated (cudaDeviceReset) cannot leave a stale address behind; while
+// the stream is capturing, the address of the last uncaptured call on this
+// device is used, so such a call must come first.
+msf_status scratch_address(int device, cudaStream_t s, unsigned char** out) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    msf::set_error("msf_probe_noalloc: cudaStreamIsCapturing failed");
+    return MSF_ERR_CUDA;
+  }
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_address[device]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, msf_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -59,6 +74,10 @@ msf_status scratch_address(int device, unsigned char** out) {
       return MSF_ERR_CUDA;
     }
     g_address[device] = p;
+  } else if (!g_address[device]) {
+    msf::set_error("msf_probe_noalloc: the first call on a device must not be captured "
+                   "(the scratch address is looked up outside a capture)");
+    return MSF_ERR_ARG;
   }
   *out = static_cast<unsigned char*>(g_address[device]);
   return MSF_OK;
@@ -128,15 +147,15 @@ extern "C" msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* 
     msf::set_error("msf_probe_noalloc: device ordinal out of range");
     return MSF_ERR_ARG;
   }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   unsigned char* base = nullptr;
-  msf_status st = scratch_address(device, &base);
+  msf_status st = scratch_address(device, s, &base);
   if (st != MSF_OK) return st;
   double* kx = reinterpret_cast<double*>(base);
   double* ky = reinterpret_cast<double*>(base + kDomainBytes);
   double2* twx = reinterpret_cast<double2*>(base + 2 * kDomainBytes);
   double2* twy = reinterpret_cast<double2*>(base + 2 * kDomainBytes + kTwiddleBytes);
   double* norm = reinterpret_cast<double*>(base + 2 * kDomainBytes + 2 * kTwiddleBytes);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   // scalars of tem.cpp:424-788 (no host allocation)
   const int dxf = grid->dupe_x > 0 ? grid->dupe_x : 1, dyf = grid->dupe_y > 0 ? grid->dupe_y : 1;

@@ -50,15 +50,16 @@ def case_dir(name, tmp_root: Path) -> Path:
     if meta["committed_specimen"]:
         shutil.copy(GOLDEN / meta["argv"][1], target)
     else:
-        if name not in _SPEC_CACHE:
+        key = json.dumps(meta["recipe"], sort_keys=True)  # cases may share a specimen
+        if key not in _SPEC_CACHE:
             sys.path.insert(0, str(GOLDEN))
             import make_golden  # the recipe that made the fixture
             gen = tmp_root / ("_gen_" + name + ".data")
             make_golden.make_specimen_file(meta["recipe"], gen)
             digest = hashlib.sha256(gen.read_bytes()).hexdigest()
             assert digest == meta["specimen_sha256"], "regenerated specimen differs"
-            _SPEC_CACHE[name] = gen
-        shutil.copy(_SPEC_CACHE[name], target)
+            _SPEC_CACHE[key] = gen
+        shutil.copy(_SPEC_CACHE[key], target)
     files = meta.get("files", {})
     for fname, text in files.items():  # parameter / MTF files, names made absolute
         for other in files:

@@ -61,6 +61,29 @@ def test_noalloc_probe_matches_allocating_entry_point_twice():
         np.testing.assert_allclose((got ** 2).sum(), 1.0, rtol=1e-12)
 
 
+@pytest.mark.parametrize("nx,ny", [(2048, 2048), (2048, 64)])
+def test_noalloc_probe_at_its_size_limit(nx, ny):
+    """At the documented limit of 2048 samples the scratch is used in full
+    and the FP64 row and column transforms need their large shared-memory
+    launches; the result must still match msf_probe."""
+    import torch
+
+    lib = msf.lib()
+    lam, _ = msf.wavelength(300000.0)
+    grid = _grid(nx, ny, nx * 0.0977, ny * 0.0977, 300000.0)
+    optics = msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0,
+                        defocus=0.87 * np.sqrt(1.3e7 * lam), alpha_max=0.0084)
+    out = torch.full((2 * nx * ny,), float("nan"), dtype=torch.float64, device="cuda")
+    rc = lib.msf_probe_noalloc(C.byref(grid), C.byref(optics), C.c_void_p(out.data_ptr()),
+                               C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, lib.msf_last_error().decode()
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(nx, ny, 2)
+    want = _reference_probe(grid, optics)
+    assert np.isfinite(got).all()
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+
+
 def test_noalloc_probe_rejects_grids_beyond_its_scratch():
     import torch
 
