@@ -54,6 +54,17 @@ def make_specimen(path):
     specimen.make_specimen(path, WORKLOAD["n_atoms"], WORKLOAD["box"], seed=WORKLOAD["seed"])
 
 
+def fp32_peak_tflops(device, sm_max_mhz):
+    """FP32 CUDA-core peak of the device: SMs x 128 FP32 lanes x 2 flops
+    (FMA) x the maximum SM clock (computed from the part's description)."""
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+    except Exception:
+        sms = 148
+    return sms * 128 * 2 * sm_max_mhz * 1e6 / 1e12
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -636,8 +647,20 @@ def main():
     traffic = ncu_traffic(dom) if (n == 1024 and args.precision == "fp32") else None
     if traffic is not None:
         traffic *= nb / 32.0
+    # the flop ceiling beside the HBM one: two complex 2-D FFTs at
+    # 5 n log2 n plus the point-wise work, per probe*slice, against the
+    # FP32 CUDA-core peak (SMs x 128 lanes x 2 flops x max SM clock;
+    # computed, not measured -- the FFT does not run on tensor cores)
+    flops_ps = 10.0 * n * n * math.log2(float(n * n)) + 20.0 * n * n
+    sm_max = clocks.summary().get("sm_max_mhz") or 1965.0
+    fp32_peak = fp32_peak_tflops(local, sm_max)
+    flop_rate = value / world * flops_ps / 1e12
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
+                "flops_per_probe_slice": flops_ps,
+                "flop_achieved_tflops_per_gpu": round(flop_rate, 2),
+                "fp32_peak_tflops": round(fp32_peak, 1),
+                "flop_frac": round(flop_rate / fp32_peak, 4),
                 "kernel": "%s pass (fused FFT + %s), %d probes/launch" %
                           (dom, "transmission" if dom == "row" else "propagator", nb),
                 "peak_source": peak_kind, "ms_row": round(ms_row, 4), "ms_col": round(ms_col, 4),
@@ -681,7 +704,17 @@ def main():
         sample[sample.index("--rasterspacing") + 1] = repr(WORKLOAD["box"][0] / 8)
         plain, fused_1, v_err, fp64_rate = plain_and_precision(msf, job, q, z, local, sample,
                                                                last)
-        versus = {"plain_gpu": {"value": round(plain, 1), "unit": UNIT,
+        need = 50.0 * plain * flops_ps / 1e12
+        versus = {"target_50x_plain": {
+                      "value": round(50.0 * plain, 1), "unit": UNIT,
+                      "flops_needed_tflops": round(need, 1),
+                      "fp32_peak_tflops": round(fp32_peak, 1),
+                      "reachable": need <= fp32_peak,
+                      "why": "50x the plain path needs %.0f TFLOP/s of FFT arithmetic, "
+                             "%.1fx the FP32 CUDA-core peak; the FFT is not a dense "
+                             "contraction and runs without tensor cores" %
+                             (need, need / fp32_peak)},
+                  "plain_gpu": {"value": round(plain, 1), "unit": UNIT,
                                 "path": "msf_run_plain: FP64, one probe at a time, one launch "
                                         "per reference step, no CUDA graph",
                                 "sample": "8x8 raster of the same specimen"},

@@ -366,6 +366,14 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
       }
       MSF_TRY(upload(ctx, &spec->dead_bits, bits));
       MSF_TRY(upload(ctx, &spec->live_groups, groups));
+      const int T1 = fp ? 0 : staged_row_threads(g.ny, 1);
+      if (T1 > 0) {  // the same bits for the staged row pass's schedule 1
+        std::vector<uint32_t> bits1(T1, 0u);
+        for (int t = 0; t < T1; ++t)
+          for (int m = 0; m < g.ny / T1; ++m)
+            if (dead[t + T1 * m]) bits1[t] |= 1u << m;
+        MSF_TRY(upload(ctx, &spec->dead_bits_alt, bits1));
+      }
       spec->n_live_groups = (int)groups.size();
       spec->h_dead_bits = bits;
       spec->h_live_groups = groups;
@@ -504,7 +512,10 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   col.py = static_cast<const char*>(spec->prop.p) + cbytes * g.nx;
   // the same kernels run_raster launches for slices after the first
   const int pipe = ctx->pipe_for(g.nx, g.ny);
-  const bool pipe_row = !fp64 && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
+  const bool staged_row = !fp64 && staged_row_supported(g.nx, g.ny) && (pipe & MSF_ROW_STAGED);
+  const int row_sched = staged_row && (pipe & MSF_ROW_ALT) ? 1 : 0;
+  const bool pipe_row =
+      !fp64 && !staged_row && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
   const bool pipe_col = pipe_supported(g.nx, g.ny, fp64) && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
@@ -517,9 +528,13 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
     col.live_groups = spec->live_groups.as<int32_t>();
     col.n_live_groups = spec->n_live_groups;
   }
+  PassArgs row_staged = row;  // schedule 1 reads the zero bits in its own layout
+  if (row_sched == 1 && row.row_dead_bits) row_staged.row_dead_bits = spec->dead_bits_alt.as<uint32_t>();
   auto row_pass = [&]() {
-    return pipe_row ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
-                    : launch_row(fp64, rop, row, ctx->stream);
+    return staged_row ? launch_row_split_staged(row_staged, d_err.as<int>(), ctx->stream,
+                                                row_sched)
+           : pipe_row ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
+                      : launch_row(fp64, rop, row, ctx->stream);
   };
   auto col_pass = [&]() {
     return pipe_col ? launch_col_slice_pipe(col, false, col_map, d_err.as<int>(), ctx->stream, fp64)
@@ -1025,7 +1040,10 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
 
   // persistent TMA-pipelined passes for FP32 grids they support
   const int pipe = ctx->pipe_for(g.nx, g.ny);
-  const bool pipe_row = !fp64 && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
+  const bool staged_row = !fp64 && staged_row_supported(g.nx, g.ny) && (pipe & MSF_ROW_STAGED);
+  const int row_sched = staged_row && (pipe & MSF_ROW_ALT) ? 1 : 0;
+  const bool pipe_row =
+      !fp64 && !staged_row && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
   const bool pipe_col = pipe_supported(g.nx, g.ny, fp64) && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
@@ -1083,7 +1101,12 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
         op = s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT;
         row.psi0 = P.psi0_tab.as<float>() + 2 * plane * s;
       }
-      if (pipe_row && op == ROW_SPLIT)
+      if (staged_row && op == ROW_SPLIT) {
+        PassArgs rs = row;  // schedule 1 reads the zero bits in its own layout
+        if (row_sched == 1 && rs.row_dead_bits) rs.row_dead_bits = spec->dead_bits_alt.as<uint32_t>();
+        MSF_CUDA(launch_row_split_staged(rs, d_err.as<int>(), ctx->stream, row_sched));
+      }
+      else if (pipe_row && op == ROW_SPLIT)
         MSF_CUDA(launch_row_split_pipe(row, d_err.as<int>(), ctx->stream));
       else
         MSF_CUDA(launch_row(fp64, op, row, ctx->stream));

@@ -65,15 +65,22 @@ struct DevBuf {
 
 }  // namespace msf
 
-constexpr int MSF_PIPE_COL = 1, MSF_PIPE_ROW = 2;
+// Slice-pass variants (bit mask): the persistent TMA-pipelined column pass,
+// the persistent pipelined split-wave row pass, and the split-wave row pass
+// with its transmission and vacuum rows staged in shared memory by bulk
+// copies (which takes precedence over MSF_PIPE_ROW).
+constexpr int MSF_PIPE_COL = 1, MSF_PIPE_ROW = 2, MSF_ROW_STAGED = 4;
+// with MSF_ROW_STAGED: the row pass's alternative FFT radix schedule
+constexpr int MSF_ROW_ALT = 8;
+constexpr int MSF_PIPE_ALL = MSF_PIPE_COL | MSF_PIPE_ROW | MSF_ROW_STAGED | MSF_ROW_ALT;
 
 struct msf_context {
   int device = 0;
   bool fp64 = true;
   int batch = 0;
   bool graphs = true;
-  // persistent TMA-pipelined FP32 passes: bit mask of MSF_PIPE_COL and
-  // MSF_PIPE_ROW, overridden by the MSF_PIPE environment variable
+  // slice-pass variants: bit mask of MSF_PIPE_COL, MSF_PIPE_ROW and
+  // MSF_ROW_STAGED, overridden by the MSF_PIPE environment variable
   int pipe = MSF_PIPE_COL;
   // slice potentials: 0 FFT convolution for slices of at least 64 atoms,
   // direct sum otherwise; 1 always direct; 2 always FFT (MSF_POTENTIAL =
@@ -118,6 +125,9 @@ struct msf_specimen {
   // columns the band limit removes entirely: row-pass zero bits, and the
   // column groups of the pipelined column pass that keep any column
   msf::DevBuf dead_bits, live_groups;
+  // the row-pass zero bits in the layout of the alternative FFT schedule of
+  // the staged row pass (FP32 contexts; empty when it does not apply)
+  msf::DevBuf dead_bits_alt;
   std::vector<uint32_t> h_dead_bits;  // host copies (slot lanes compare them)
   std::vector<int32_t> h_live_groups;
   int n_live_groups = 0, n_live_columns = 0;

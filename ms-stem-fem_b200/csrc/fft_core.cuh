@@ -58,6 +58,23 @@ template <> __device__ __forceinline__ float2 cscale<float2, float>(float2 a, fl
 }
 #endif
 
+// Split-wave transmission update of one element.  psi = psi0 + d with
+// psi0 the vacuum wave and t = 1 + tau; the reference's in-place update
+// (adfstem.cpp:1929-1949)
+//   re' = (tr*re - ti*im)/s,  im' = (tr*im + ti*re')/s
+// is linear over the reals, so the scattered part evolves as
+//   dre' = (tau_r*p0r - ti*p0i + (1+tau_r)*dre - ti*dim)/s
+//   dim' = (tau_r*p0i + (1+tau_r)*dim + ti*(p0r/s + dre'))/s
+// with every term formed at the scale of d, not of psi0.  Every split-wave
+// row pass calls this one function, so they agree bit for bit.
+template <typename C, typename Real>
+__device__ __forceinline__ C split_elem(C p0, C tau, C d, Real is) {
+  const Real dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
+  const Real re_total = p0.x * is + dre;
+  const Real dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
+  return C{dre, dim};
+}
+
 template <int I> using ic = std::integral_constant<int, I>;
 
 // Loads issued between two fences may be scheduled together; a fence keeps
@@ -138,10 +155,14 @@ __device__ __forceinline__ void dft(C (&v)[E]) {
 
 // ---------------------------------------------------------------- shapes --
 // FFT length N: E elements per thread, S radix stages R0..R{S-1} (each R
-// divides E).  FP64 keeps E <= 16 to bound register use.
-template <int N, typename Real> struct Shape;
-#define MSF_SHAPE(N_, REAL_, E_, S_, R0_, R1_, R2_)                          \
-  template <> struct Shape<N_, REAL_> {                                       \
+// divides E).  FP64 keeps E <= 16 to bound register use.  V selects the
+// radix schedule: V = 0 is the default of every kernel; V = 1 is the
+// alternative schedule of the FP32 split-wave row pass at 256..2048 points
+// (half the elements per thread, twice the threads per line, one more
+// radix stage), which the launch autotuner times against V = 0 per grid.
+template <int N, typename Real, int V = 0> struct Shape;
+#define MSF_SHAPE(N_, REAL_, V_, E_, S_, R0_, R1_, R2_)                      \
+  template <> struct Shape<N_, REAL_, V_> {                                   \
     static constexpr int N = N_, E = E_, S = S_, T = N_ / E_;                 \
     static constexpr int R0 = R0_, R1 = R1_, R2 = R2_;                        \
     __host__ __device__ static constexpr int radix(int s) { return s == 0 ? R0 : s == 1 ? R1 : R2; } \
@@ -149,29 +170,24 @@ template <int N, typename Real> struct Shape;
       return s == 0 ? 1 : s == 1 ? R0 : R0 * R1;                              \
     }                                                                         \
   };
-MSF_SHAPE(64, float, 8, 2, 8, 8, 1)
-MSF_SHAPE(128, float, 16, 2, 16, 8, 1)
-MSF_SHAPE(256, float, 16, 2, 16, 16, 1)
-#ifndef MSF_F32_WIDE
-#define MSF_F32_WIDE 1
-#endif
-#if MSF_F32_WIDE
-MSF_SHAPE(512, float, 32, 2, 32, 16, 1)
-MSF_SHAPE(1024, float, 32, 2, 32, 32, 1)
-MSF_SHAPE(2048, float, 32, 3, 32, 8, 8)
-#else
-MSF_SHAPE(512, float, 16, 3, 16, 16, 2)
-MSF_SHAPE(1024, float, 16, 3, 16, 16, 4)
-MSF_SHAPE(2048, float, 16, 3, 16, 16, 8)
-#endif
-MSF_SHAPE(4096, float, 16, 3, 16, 16, 16)
-MSF_SHAPE(64, double, 8, 2, 8, 8, 1)
-MSF_SHAPE(128, double, 16, 2, 16, 8, 1)
-MSF_SHAPE(256, double, 16, 2, 16, 16, 1)
-MSF_SHAPE(512, double, 8, 3, 8, 8, 8)
-MSF_SHAPE(1024, double, 16, 3, 16, 16, 4)
-MSF_SHAPE(2048, double, 16, 3, 16, 16, 8)
-MSF_SHAPE(4096, double, 16, 3, 16, 16, 16)
+MSF_SHAPE(64, float, 0, 8, 2, 8, 8, 1)
+MSF_SHAPE(128, float, 0, 16, 2, 16, 8, 1)
+MSF_SHAPE(256, float, 0, 16, 2, 16, 16, 1)
+MSF_SHAPE(512, float, 0, 32, 2, 32, 16, 1)
+MSF_SHAPE(1024, float, 0, 32, 2, 32, 32, 1)
+MSF_SHAPE(2048, float, 0, 32, 3, 32, 8, 8)
+MSF_SHAPE(4096, float, 0, 16, 3, 16, 16, 16)
+MSF_SHAPE(256, float, 1, 8, 3, 8, 8, 4)
+MSF_SHAPE(512, float, 1, 16, 3, 16, 16, 2)
+MSF_SHAPE(1024, float, 1, 16, 3, 16, 16, 4)
+MSF_SHAPE(2048, float, 1, 16, 3, 16, 16, 8)
+MSF_SHAPE(64, double, 0, 8, 2, 8, 8, 1)
+MSF_SHAPE(128, double, 0, 16, 2, 16, 8, 1)
+MSF_SHAPE(256, double, 0, 16, 2, 16, 16, 1)
+MSF_SHAPE(512, double, 0, 8, 3, 8, 8, 8)
+MSF_SHAPE(1024, double, 0, 16, 3, 16, 16, 4)
+MSF_SHAPE(2048, double, 0, 16, 3, 16, 16, 8)
+MSF_SHAPE(4096, double, 0, 16, 3, 16, 16, 16)
 #undef MSF_SHAPE
 
 // Worst bank multiplicity of one shared-memory access phase (128 bytes of

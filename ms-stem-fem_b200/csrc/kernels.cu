@@ -91,15 +91,9 @@ constexpr int col_cols() {
 }
 
 // ------------------------------------------------------------ row pass ---
-// Split-wave transmission step on one row held in registers (element
-// t + T*m of row i).  psi = psi0 + delta with psi0 the probe's vacuum wave
-// (shifted like the probe) and t = 1 + tau.  The reference's update
-// (adfstem.cpp:1929-1949)
-//   re' = (tr*re - ti*im)/s,  im' = (tr*im + ti*re')/s
-// is linear over the reals, so the scattered part evolves as
-//   dre' = (tau_r*p0r - ti*p0i + (1+tau_r)*dre - ti*dim)/s
-//   dim' = (tau_r*p0i + (1+tau_r)*dim + ti*(p0r/s + dre'))/s
-// and every term is formed at the scale of delta, not of psi0.
+// Split-wave transmission step (split_elem) on one row held in registers
+// (element t + T*m of row i); psi0 is the probe's vacuum wave, shifted like
+// the probe.
 template <typename Sh, typename C, typename Real>
 __device__ __forceinline__ void split_update(C (&v)[Sh::E], const C* __restrict__ psi0,
                                              const C* __restrict__ trans, int nx, int i,
@@ -115,11 +109,7 @@ __device__ __forceinline__ void split_update(C (&v)[Sh::E], const C* __restrict_
     const int iy = (y < sy) ? y + N - sy : y - sy;
     const C p0 = __ldg(prow + iy);
     const C tau = __ldg(trow + y);
-    const C d = v[m];
-    const Real dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
-    const Real re_total = p0.x * is + dre;
-    const Real dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
-    v[m] = C{dre, dim};
+    v[m] = split_elem(p0, tau, v[m], is);
   }
 }
 
@@ -336,13 +326,10 @@ cudaError_t row_launch(const PassArgs& a, cudaStream_t s) {
   constexpr int L = row_lines<Real, N>();
   using Sh = Shape<N, Real>;
   constexpr int smem = L * Smem<Sh, (int)sizeof(Cx<Real>), L, false>::stride * (int)sizeof(Cx<Real>);
-  static bool configured = false;
+  static PerDevice configured;
   auto k = row_kernel<Real, N, L, OP>;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  if (cudaError_t e = smem_limit_once((const void*)k, smem, configured); e != cudaSuccess)
+    return e;
   if (a.nx % L != 0) return cudaErrorInvalidValue;
   int groups = a.nx / L;
   if constexpr (OP == ROW_SLOTS) {
@@ -361,13 +348,10 @@ cudaError_t col_launch(const PassArgs& a, cudaStream_t s) {
   constexpr int CC = col_cols<Real, N>();
   using Sh = Shape<N, Real>;
   constexpr int smem = CC * Smem<Sh, (int)sizeof(Cx<Real>), CC, true>::stride * (int)sizeof(Cx<Real>);
-  static bool configured = false;
+  static PerDevice configured;
   auto k = col_kernel<Real, N, CC, OP>;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  if (cudaError_t e = smem_limit_once((const void*)k, smem, configured); e != cudaSuccess)
+    return e;
   if (a.ny % CC != 0) return cudaErrorInvalidValue;
   dim3 grid(a.nb, a.ny / CC);
   k<<<grid, CC * Sh::T, smem, s>>>(a);
@@ -906,6 +890,19 @@ inline unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1)
 
 }  // namespace
 
+// SMs of the current device (cached per device ordinal)
+int sm_count() {
+  static std::atomic<int> cached[64];
+  const int dev = current_device();
+  int n = (dev >= 0 && dev < 64) ? cached[dev].load() : 0;
+  if (n <= 0) {
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev < 0 ? 0 : dev);
+    if (n <= 0) n = 1;
+    if (dev >= 0 && dev < 64) cached[dev].store(n);
+  }
+  return n;
+}
+
 bool supported_length(int n) {
   return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096;
 }
@@ -1120,13 +1117,7 @@ cudaError_t launch_propagate(double* psi, const double* px, const double* py, co
 cudaError_t launch_slot_detect(const void* table, int max_done, int max_chunks, int nx, int ny,
                                double* partial, bool pixel_sums, cudaStream_t s) {
   if (max_done <= 0 || max_chunks <= 0) return cudaErrorInvalidValue;
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 1;
-  }
+  const int sms = sm_count();
   double* pa = partial;
   double* pi = partial + (int64_t)max_done * max_chunks;
   slot_chunk_kernel<<<4 * sms, 256, 0, s>>>(table, max_chunks, nx, ny, pa, pi);

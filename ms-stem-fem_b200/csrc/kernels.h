@@ -2,10 +2,43 @@
 // No CUDA types beyond cudaStream_t cross this header; all device pointers
 // are passed as void* / typed raw pointers owned by the caller.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace msf {
+
+// Launch set-up that is per device (cudaFuncSetAttribute, occupancy):
+// each launcher keeps one bit per device ordinal, so a process that uses
+// several devices configures every one of them, and threads that race on
+// the first launch of a device both do the (idempotent) set-up.  Ordinals
+// past 63 redo the set-up on every launch.
+struct PerDevice {
+  std::atomic<uint64_t> bits{0};
+  bool needed(int dev) const {
+    return dev < 0 || dev >= 64 || !((bits.load(std::memory_order_acquire) >> dev) & 1u);
+  }
+  void mark(int dev) {
+    if (dev >= 0 && dev < 64) bits.fetch_or(uint64_t(1) << dev, std::memory_order_release);
+  }
+};
+inline int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) return -1;
+  return d;
+}
+// SMs of the current device (cached per device ordinal).
+int sm_count();
+// Raise `func`'s dynamic shared-memory limit to `bytes` on the current
+// device, once per device.
+inline cudaError_t smem_limit_once(const void* func, int bytes, PerDevice& once) {
+  const int dev = current_device();
+  if (!once.needed(dev)) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) once.mark(dev);
+  return e;
+}
 
 // Which fused operation a row pass (transform along y, contiguous) does.
 enum RowOp : int {
@@ -115,6 +148,21 @@ bool pipe_supported(int nx, int ny, bool fp64 = false);
 // Split-wave row pass for slices after the first; *err set to 1 if a copy
 // never arrived (bounded wait).
 cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s);
+// Split-wave row pass for slices after the first with the slice tables
+// staged: each CTA transforms one row of several probes and bulk-copies
+// the shared transmission row and the probes' vacuum rows into shared
+// memory during the inverse transform (FP32, row lengths 256..2048).
+// Honours row_dead_bits / row_dead_io like launch_row (with the bit layout
+// of the schedule's threads per line); *err set to 1 if a copy never
+// arrived (bounded wait).  `schedule` picks the FFT radix schedule: 0 the
+// default (32 elements a thread from 512 points), 1 half the elements and
+// twice the threads per line.  Bit-identical to launch_row's ROW_SPLIT
+// with schedule 0; schedule 1 rounds differently (another factorisation).
+bool staged_row_supported(int nx, int ny);
+// Threads per line of the staged row pass's transform (0 if unsupported).
+int staged_row_threads(int ny, int schedule);
+cudaError_t launch_row_split_staged(const PassArgs& a, int* err, cudaStream_t s,
+                                    int schedule = 0);
 // Column slice pass (COL_SLICE, or COL_SLICE_LAST when `last`; per slot
 // when a.slots is set); `tensor_map` from encode_column_map over the same
 // batch buffer.

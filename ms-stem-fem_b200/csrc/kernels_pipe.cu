@@ -70,6 +70,13 @@ __device__ __forceinline__ void tile_g2s(void* dst, const CUtensorMap* map, int 
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+// A wavefield element loaded once per pass: not allocated in L1, which
+// then keeps the twiddle table (read by every stage of every line).
+__device__ __forceinline__ float2 ld_once(const float2* p) {
+  float2 v;
+  asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -160,11 +167,7 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
       const int iy = (y < sy) ? y + N - sy : y - sy;
       const C p0 = __ldg(prow + iy);
       const C tau = __ldg(trow + y);
-      const C d = v[m];
-      const float dre = (tau.x * p0.x - tau.y * p0.y + d.x + tau.x * d.x - tau.y * d.y) * is;
-      const float re_total = p0.x * is + dre;
-      const float dim = (tau.x * p0.y + d.y + tau.x * d.y + tau.y * re_total) * is;
-      v[m] = C{dre, dim};
+      v[m] = split_elem(p0, tau, v[m], is);
     }
     fft_line<Sh, false>(v, sm, t, tw, sync);
     C* row = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)i * N;
@@ -176,6 +179,129 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
       issue(item + 2 * gridDim.x, w);
     }
   }
+}
+
+// -------------------------------------------- row pass (split, staged) --
+// The split-wave row pass with its slice tables staged in shared memory.
+// One CTA transforms row i of P probes of the batch (one line each).  On
+// entry thread 0 starts bulk copies of the transmission row tau[i], which
+// the P lines share, and of each probe's vacuum row psi0[(i - sx) mod nx];
+// meanwhile every line loads its scattered row from global memory and runs
+// the inverse transform, so the update then reads tau and psi0 from shared
+// memory with no L2 round trip left on its path.  Arithmetic is that of
+// ROW_SPLIT (split_elem) element for element, so the results are
+// bit-identical.  A probe index past the batch leaves its line idle (it
+// still takes part in the barriers of a line that spans two warps).  V is
+// the FFT radix schedule (Shape<N, float, V>).
+template <int N, int V>
+constexpr int staged_lines() {
+  constexpr int T = Shape<N, float, V>::T;
+  return T >= 128 ? 1 : 128 / T;
+}
+template <int N, int V>
+constexpr int staged_min_ctas() {
+  // schedule 0 (32 elements a thread): 384 threads per SM (168 registers)
+  // up to 1024-point lines, 256 for 2048-point lines, whose transforms need
+  // 255 registers; schedule 1 (16 or 8 elements): 512 (128 registers)
+  constexpr int per_sm = V == 1 ? 512 : (N >= 2048 ? 256 : 384);
+  return per_sm / (staged_lines<N, V>() * Shape<N, float, V>::T);
+}
+template <int N, int V>
+constexpr int staged_smem() {
+  using SM = Smem<Shape<N, float, V>, 8, staged_lines<N, V>(), false>;
+  return (N + staged_lines<N, V>() * N + staged_lines<N, V>() * SM::stride) * 8;
+}
+
+template <int N, int P, int V>
+__global__ void __launch_bounds__(P * Shape<N, float, V>::T, staged_min_ctas<N, V>())
+row_split_staged_kernel(const PassArgs a, int* err) {
+  using C = float2;
+  using Sh = Shape<N, float, V>;
+  using SM = Smem<Sh, 8, P, false>;
+  constexpr int E = Sh::E, T = Sh::T;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C* tau_s = reinterpret_cast<C*>(smem_raw);  // [N]
+  C* psi0_s = tau_s + N;                      // [P][N]
+  C* exch = psi0_s + P * N;                   // [P][SM::stride]
+  __shared__ uint64_t bar;
+  __shared__ int flag;
+  const int line = threadIdx.x / T, t = threadIdx.x % T;
+  const int i = blockIdx.y;
+  const int b0 = blockIdx.x * P;
+  const int b = b0 + line;
+  const int nvalid = a.nb - b0 < P ? a.nb - b0 : P;
+  const bool valid = line < nvalid;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    mbar_expect_tx(&bar, (uint32_t)((1 + nvalid) * N * 8));
+    bulk_g2s(tau_s, static_cast<const C*>(a.trans) + (int64_t)i * N, N * 8, &bar);
+    for (int l = 0; l < nvalid; ++l) {
+      const int sx = a.shifts[2 * (b0 + l)];
+      const int ix = (i < sx) ? i + a.nx - sx : i - sx;
+      bulk_g2s(psi0_s + l * N, static_cast<const C*>(a.psi0) + (int64_t)ix * N, N * 8, &bar);
+    }
+  }
+  __syncthreads();
+  auto sync = [] {
+    if constexpr (T <= 32) __syncwarp();
+    else __syncthreads();
+  };
+  C* row = static_cast<C*>(a.psi) + (int64_t)(valid ? b : 0) * a.batch_stride + (int64_t)i * N;
+  const C* tw = static_cast<const C*>(a.tw);
+  // columns removed by the band limit were not stored: they are zero
+  const uint32_t dead = a.row_dead_bits ? __ldg(a.row_dead_bits + t) : 0u;
+  const uint32_t skip = (a.row_dead_io & 1) ? dead : 0u;
+  C v[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m)
+    v[m] = (!valid || ((skip >> m) & 1u)) ? C{0.f, 0.f} : ld_once(row + t + T * m);
+  C* sm = exch + line * SM::stride;
+  fft_line<Sh, true>(v, sm, t, tw, sync);
+  // wait (bounded) for the staged rows: warp-uniform for lines within a
+  // warp, CTA-uniform for lines that span warps (they share barriers)
+  bool ok;
+  if constexpr (T <= 32) {
+    int r = 0;
+    if ((threadIdx.x & 31) == 0) r = mbar_wait_bounded(&bar, 0) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, r, 0) != 0;
+    if (ok) mbar_wait_bounded(&bar, 0);  // every thread observes the phase
+  } else {
+    ok = cta_wait(&bar, 0, &flag);
+  }
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      atomicExch(err, 1);
+      mbar_wait_bounded(&bar, 0);  // the copies may still be landing
+    }
+    return;
+  }
+  if (valid) {
+    const int sy = a.shifts[2 * b + 1];
+    const C* p0 = psi0_s + line * N;
+    const float is = (float)a.inv_s;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int y = t + T * m;
+      const int iy = (y < sy) ? y + N - sy : y - sy;
+      v[m] = split_elem(p0[iy], tau_s[y], v[m], is);
+    }
+  }
+  fft_line<Sh, false>(v, sm, t, tw, sync);
+  if (!valid) return;
+  if (a.row_dead_bits) {  // columns the next band limit removes entirely
+    if (a.row_dead_io & 2) {  // nobody reads them: leave them unstored
+#pragma unroll
+      for (int m = 0; m < E; ++m)
+        if (!((dead >> m) & 1u)) row[t + T * m] = v[m];
+      return;
+    }
+#pragma unroll
+    for (int m = 0; m < E; ++m)
+      if ((dead >> m) & 1u) v[m] = C{0.f, 0.f};
+  }
+#pragma unroll
+  for (int m = 0; m < E; ++m) row[t + T * m] = v[m];
 }
 
 // ----------------------------------------------------- column slice pass --
@@ -306,16 +432,6 @@ col_slice_pipe_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tmap
   }
 }
 
-int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 1;
-  }
-  return n;
-}
 
 template <int N>
 constexpr int pipe_lines() { return 256 / Shape<N, float>::T; }
@@ -336,16 +452,37 @@ cudaError_t row_pipe_launch(const PassArgs& a, int* err, cudaStream_t s) {
   constexpr int L = pipe_lines<N>();
   using SM = Smem<Shape<N, float>, 8, L, false>;
   constexpr int smem = 2 * L * SM::stride * 8;
-  static bool configured = false;
+  static PerDevice configured;
   auto k = row_split_pipe_kernel<N, L>;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  if (cudaError_t e = smem_limit_once((const void*)k, smem, configured); e != cudaSuccess)
+    return e;
   const int items = a.nb * (a.nx / L);
   const int grid = items < sm_count() ? items : sm_count();
   k<<<grid, L * Shape<N, float>::T, smem, s>>>(a, err);
+  return cudaGetLastError();
+}
+
+template <int N, int V>
+cudaError_t row_staged_launch(const PassArgs& a, int* err, cudaStream_t s) {
+  constexpr int P = staged_lines<N, V>();
+  constexpr int smem = staged_smem<N, V>();
+  static_assert(smem * staged_min_ctas<N, V>() <= 227 * 1024,
+                "staged row pass: its CTAs per SM exceed shared memory");
+  static PerDevice configured;
+  auto k = row_split_staged_kernel<N, P, V>;
+  const int dev = current_device();
+  if (configured.needed(dev)) {
+    // several CTAs per SM need the largest shared-memory carveout
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    configured.mark(dev);
+  }
+  if (a.nb <= 0) return cudaSuccess;
+  dim3 grid((a.nb + P - 1) / P, a.nx);
+  k<<<grid, P * Shape<N, float, V>::T, smem, s>>>(a, err);
   return cudaGetLastError();
 }
 
@@ -357,14 +494,20 @@ cudaError_t col_pipe_launch(const PassArgs& a, const CUtensorMap& map, int* err,
   using SM = Smem<Shape<N, Real>, CB, CC, true>;
   constexpr int RAW = (N * CC > CC * SM::stride ? N * CC : CC * SM::stride);
   constexpr int smem = 2 * ((RAW + 15) / 16 * 16) * CB;
-  static int per_sm = 0;
+  // resident CTAs per SM, found once per device after raising the limit
+  static PerDevice configured;
+  static std::atomic<int> per_sm_dev[64];
   auto k = col_slice_pipe_kernel<Real, N, CC, LAST, SLOTS>;
-  if (!per_sm) {
+  const int dev = current_device();
+  int per_sm = (dev >= 0 && dev < 64) ? per_sm_dev[dev].load() : 0;
+  if (configured.needed(dev) || per_sm < 1) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, CC * Shape<N, Real>::T, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
+    if (dev >= 0 && dev < 64) per_sm_dev[dev].store(per_sm);
+    configured.mark(dev);
   }
   const int items = a.nb * (a.live_groups ? a.n_live_groups : a.ny / CC);
   if (items <= 0) return cudaSuccess;
@@ -407,6 +550,40 @@ cudaError_t launch_row_split_pipe(const PassArgs& a, int* err, cudaStream_t s) {
     case 512: return row_pipe_launch<512>(a, err, s);
     case 1024: return row_pipe_launch<1024>(a, err, s);
     case 2048: return row_pipe_launch<2048>(a, err, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+bool staged_row_supported(int nx, int ny) {
+  (void)nx;
+  return ny == 256 || ny == 512 || ny == 1024 || ny == 2048;
+}
+
+int staged_row_threads(int ny, int schedule) {
+  switch (ny) {
+    case 256: return schedule ? Shape<256, float, 1>::T : Shape<256, float>::T;
+    case 512: return schedule ? Shape<512, float, 1>::T : Shape<512, float>::T;
+    case 1024: return schedule ? Shape<1024, float, 1>::T : Shape<1024, float>::T;
+    case 2048: return schedule ? Shape<2048, float, 1>::T : Shape<2048, float>::T;
+  }
+  return 0;
+}
+
+cudaError_t launch_row_split_staged(const PassArgs& a, int* err, cudaStream_t s, int schedule) {
+  if (schedule == 1) {
+    switch (a.ny) {
+      case 256: return row_staged_launch<256, 1>(a, err, s);
+      case 512: return row_staged_launch<512, 1>(a, err, s);
+      case 1024: return row_staged_launch<1024, 1>(a, err, s);
+      case 2048: return row_staged_launch<2048, 1>(a, err, s);
+    }
+    return cudaErrorInvalidValue;
+  }
+  switch (a.ny) {
+    case 256: return row_staged_launch<256, 0>(a, err, s);
+    case 512: return row_staged_launch<512, 0>(a, err, s);
+    case 1024: return row_staged_launch<1024, 0>(a, err, s);
+    case 2048: return row_staged_launch<2048, 0>(a, err, s);
   }
   return cudaErrorInvalidValue;
 }

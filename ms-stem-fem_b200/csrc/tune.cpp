@@ -1,10 +1,11 @@
 // Launch tiling autotuner.  The reference plans its FFTs with FFTW_MEASURE
 // and keeps the plans as a wisdom file per grid (tem.cpp:583-616, exported
-// at 1748-1765).  Here the FFT radix schedule is fixed per length at compile
-// time; what is measured per grid is the tiling of the batched slice
-// passes: probes per launch and whether the column pass runs as the
-// persistent TMA-pipelined kernel.  The winner is kept per context and can
-// be saved and reloaded as text, like wisdom.
+// at 1748-1765).  Here what is measured per grid is the tiling of the
+// batched slice passes: probes per launch, whether the column pass runs as
+// the persistent TMA-pipelined kernel, whether the split-wave row pass
+// stages its slice tables in shared memory, and that row pass's FFT radix
+// schedule (32 elements a thread in two or three stages, or 16 in three).  The winner is kept per context
+// and can be saved and reloaded as text, like wisdom.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -47,7 +48,20 @@ msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
     if ((double)cbytes * plane * b <= 0.5 * (double)free_b) batches.push_back(b);
   if (batches.empty()) batches.push_back(1);
   std::vector<int> pipes{ctx->pipe};
-  if (!ctx->pipe_env && pipe_supported(g.nx, g.ny, ctx->fp64)) pipes = {MSF_PIPE_COL, 0};
+  if (!ctx->pipe_env) {
+    const bool col = pipe_supported(g.nx, g.ny, ctx->fp64);
+    const bool staged = !ctx->fp64 && staged_row_supported(g.nx, g.ny);
+    pipes = {0};
+    if (col) pipes.push_back(MSF_PIPE_COL);
+    if (staged) {  // both FFT radix schedules of the staged row pass
+      pipes.push_back(MSF_ROW_STAGED);
+      pipes.push_back(MSF_ROW_STAGED | MSF_ROW_ALT);
+    }
+    if (col && staged) {
+      pipes.push_back(MSF_PIPE_COL | MSF_ROW_STAGED);
+      pipes.push_back(MSF_PIPE_COL | MSF_ROW_STAGED | MSF_ROW_ALT);
+    }
+  }
   const int saved_pipe = ctx->pipe;
   ctx->tuned.erase({g.nx, g.ny});  // time_passes then runs ctx->pipe
   msf_context::Tuned best;
@@ -126,7 +140,7 @@ msf_status msf_wisdom_import(msf_context* ctx, const char* text, int32_t* n_impo
     if (prec != (ctx->fp64 ? "fp64" : "fp32") || nx <= 0 || ny <= 0 || batch <= 0) continue;
     msf_context::Tuned t;
     t.batch = batch;
-    t.pipe = pipe & (MSF_PIPE_COL | MSF_PIPE_ROW);
+    t.pipe = pipe & MSF_PIPE_ALL;
     t.ns_per_probe_slice = ns;
     ctx->tuned[{nx, ny}] = t;
     ++n;
