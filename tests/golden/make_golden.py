@@ -94,6 +94,11 @@ CASES = {
               "-m 2048 2048 300000 --adfstemuncorrfem --V_omega --images --cs3 1.3e7 "
               "--scherzer_defocus --scherzer_alphamax --rasterspacing 50 --minslice 2.0",
               False, None),
+    # --paptif: per slice, 16-bit images of the projected potential before
+    # the exponential (magnitude, real and imaginary parts, linear and log)
+    "paptif": (dict(n=390, box=(25, 25, 12.5), seed=11),
+               "-m 128 128 200000 --adfstemuncorr --paptif --cs3 1.3e7 --scherzer_defocus "
+               "--alphamax 0.010 --rasterspacing 12.5 --minslice 2.0", True, None),
     # detector MTF: only the parameter-file route works in the reference (its
     # --mtf_file option does not consume its argument); FEM pixel modes too
     "mtf": (dict(n=780, box=(25, 25, 25), seed=1),
@@ -214,6 +219,12 @@ def run_case(name):
             break
         for f in work.glob("*_adfstem_*corr_%s_diffraction_scalefactor_*.tif" % tag):
             out["%s_diffraction_%s" % (tag, f.stem.split("_scalefactor_")[1])] = read_tif16(f)
+    # --paptif images: magnitude and real part (the imaginary part's min/max
+    # are uninitialised in the reference, func.cpp:2063-2065, so its images
+    # are not defined and not kept)
+    for f in sorted(work.glob(name + "_pap_slice*_complex_fftw_operand_*.tif")):
+        if "_operand_im" not in f.name:
+            out["pap_" + f.stem.split("_pap_")[1]] = read_tif16(f)
     sl = np.loadtxt(work / "slices.txt", ndmin=2)
     out["slice_lower"], out["slice_thickness"], out["slice_count"] = sl[:, 0], sl[:, 1], sl[:, 2]
     if tslice is not None:
