@@ -18,11 +18,15 @@ results back.
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 Under torchrun (N ranks, one per GPU) the raster grows to (64 N) x 64 probes
-(x spacing / N) and is sharded: each rank runs its contiguous 4,096 probes,
-then the one exchange step all-gathers the per-probe detector rows and the
-per-pixel sums over NCCL and every rank finishes the FEM statistics.  Work
-per GPU is fixed, so scaling is weak; a step is timed with CUDA events around
-shard + exchange + finish, max over ranks; rank 0 prints one JSON line.
+(x spacing / N) and is sharded through the library (msf_run_sharded): each
+rank runs its contiguous 4,096 probes, then the one exchange step
+all-gathers the per-probe detector rows and the per-pixel sums over NCCL on
+device buffers and every rank finishes the FEM statistics.  The ranks join
+at MASTER_ADDR and the port after MASTER_PORT (MSF_COMM=host exchanges
+through that bootstrap instead, for ranks sharing a GPU).  Work per GPU is
+fixed, so scaling is weak; a step is timed as the rank's raster device time
+(CUDA events) + exchange + host finish, max over ranks; rank 0 prints one
+JSON line.
 """
 import argparse
 import json
@@ -333,12 +337,30 @@ def workload_batch(args, msf, local):
     return 0
 
 
+def stress_specimen(msf, path):
+    """The precision-stress specimen as the reference reads it: 600k Si at
+    seeded positions (msf_amorphous_positions, seed 4) in 200x200x300 A,
+    written with 6 decimals and parsed back by the drop-in reader."""
+    import specimen
+    box = np.array([200.0, 200.0, 300.0])
+    pos = np.minimum(np.round(msf.amorphous_positions(600000, box, 2.2, seed=4), 6),
+                     np.round(box, 6))
+    specimen.write_lammps_data(path, pos, box)
+    return msf.Job(["-a", str(path), "--output_prefix", "stress", "-m", "2048", "2048",
+                    "300000", "--adfstemuncorrfem", "--V_omega", "--images", "--cs3", "1.3e7",
+                    "--scherzer_defocus", "--scherzer_alphamax", "--rasterspacing", "50",
+                    "--minslice", "2.0"])
+
+
 def workload_stress(args, msf, local):
     """600k atoms, 200x200x300 A, 2048^2, 300 kV, 150 slices, 16x16 raster:
-    FP32 split-wave against FP64 wavefields, per-output error."""
+    FP32 split-wave against FP64 wavefields, per-output error; and both
+    precisions on a 4x4 raster against the reference's own FP64 result for
+    the same specimen (the committed fixture tests/golden/c4_r4.npz)."""
     box = (200.0, 200.0, 300.0)
-    q = msf.amorphous_positions(600000, box, 2.2, seed=4)
-    z = np.full(len(q), 14, np.uint32)
+    work = Path(tempfile.mkdtemp(prefix="msf_stress_"))
+    job4 = stress_specimen(msf, work / "c4.data")
+    q, z = job4.positions()
     lam = msf.wavelength(300000.0)[0]
     optics = msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0,
                         defocus=msf.lib().msf_scherzer(0, lam, 1.3e7),
@@ -346,15 +368,27 @@ def workload_stress(args, msf, local):
     det = msf.Detect(outputs=msf.OUT_ADF_IMAGE | msf.OUT_V_OMEGA, det_inner=0.04,
                      det_outer=0.2, dr=1.0)
     r = Raster(msf, 16, box[0])
-    out = {}
+    out, vs_ref = {}, {}
+    golden = ROOT / "tests" / "golden" / "c4_r4.npz"
+    ref = dict(np.load(golden)) if golden.exists() else None
     for prec in ("fp32", "fp64"):
         ctx = msf.Context(device=local, precision=prec)
         t0 = time.time()
-        spec = ctx.specimen(_grid(msf, 2048, box[0], box[2], voltage=300000.0), q, z)
+        spec = ctx.specimen(job4.grid, q, z)
         setup = time.time() - t0
         ctx.run(spec, optics, r.r, det)
         res = ctx.run(spec, optics, r.r, det)
         out[prec] = (res, setup, spec.slices()["n"])
+        if ref is not None:  # the reference's 4x4 raster of the same specimen
+            r4 = ctx.run(spec, job4.optics, job4.raster, job4.detect)
+            want = ref["V_omega"][:, 1]
+            m = np.isfinite(want) & (np.abs(want) > 1e-6)
+            vs_ref[prec] = {
+                "adf_image_max_rel": float(np.max(np.abs(r4.adf_image - ref["adf_image"]) /
+                                                  np.abs(ref["adf_image"]))),
+                "v_omega_max_rel": float(np.max(np.abs(r4.v["V_omega"][m] - want[m]) /
+                                                np.abs(want[m]))),
+                "v_omega_bins": int(m.sum())}
         spec.close()
         ctx.close()
     r32, r64 = out["fp32"][0], out["fp64"][0]
@@ -373,6 +407,11 @@ def workload_stress(args, msf, local):
             "fp64": {"value": round(r64.probe_slices / r64.seconds_raster, 1), "unit": UNIT,
                      "specimen_setup_s": round(out["fp64"][1], 2)},
             "error_fp32_vs_fp64": {"adf_image_max_rel": adf_err, "v_omega_max_rel": v_err},
+            "error_vs_reference": dict(vs_ref, raster="4x4 (rasterspacing 50 A)",
+                                       bins="V_omega bins above 1e-6",
+                                       reference="the reference's own sources, FP64, FFTW "
+                                                 "replaced by an FP64 radix-2 shim") if vs_ref
+                                  else "tests/golden/c4_r4.npz absent",
             "gpu_launches": int(r32.kernel_launches)}
     print(json.dumps(line))
     return 0
@@ -436,6 +475,7 @@ def run_serving(msf, local, n_jobs, rate, slots, seed=5):
         while srv.poll(t, wait_ms=200) is None:
             pass
     st = srv.stats()
+    by_grid = srv.grid_stats()
     wall = time.time() - t_start
     srv.close()
     return {"jobs": n_jobs, "arrival_rate_per_s": rate, "slots_per_lane": slots,
@@ -445,6 +485,10 @@ def run_serving(msf, local, n_jobs, rate, slots, seed=5):
             "throughput": round(st["probe_slices"] / wall, 1), "unit": UNIT,
             "offered": round(st["probe_slices"] / max(float(gaps.sum()), 1e-9), 1),
             "wall_s": round(wall, 2),
+            "by_grid": {"%dx%d" % (g["nx"], g["ny"]): {
+                "completed": g["completed"], "p50_s": round(g["p50_s"], 3),
+                "p99_s": round(g["p99_s"], 3), "max_s": round(g["max_s"], 3)}
+                for g in by_grid},
             "mix": {str(n): sum(1 for r in reqs if r["n"] == n) for n in (256, 512, 1024, 2048)}}
 
 
@@ -494,7 +538,7 @@ def main():
                     help="requests of the second --workload serving run, at --sustained-rate")
     ap.add_argument("--sustained-rate", type=float, default=0.2,
                     help="arrivals per second one GPU sustains for the mixed stream")
-    ap.add_argument("--serving-jobs", type=int, default=8,
+    ap.add_argument("--serving-jobs", type=int, default=50,
                     help="requests of the serving sample in the headline line (0: none)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -510,21 +554,18 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    # NCCL over the GPUs by default; MSF_BENCH_DIST_BACKEND=gloo runs the same
-    # sharded flow with the exchange on the host (ranks may then share GPUs)
-    backend = os.environ.get("MSF_BENCH_DIST_BACKEND", "nccl")
-    coll_dev = "cuda" if backend == "nccl" else "cpu"
+    comm = None
     if world > 1:
-        import datetime
         import torch
-        import torch.distributed as dist
         local = local % max(1, torch.cuda.device_count())
-        torch.cuda.set_device(local)
-        # every rank runs the same collectives at most one raster step
-        # (seconds) apart: a rank that stops ends the others' next
-        # collective with an error within this bound instead of a hang
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
+        # the library's communicator: NCCL on device buffers by default;
+        # MSF_COMM=host exchanges through the bootstrap (ranks may then
+        # share a GPU).  Every wait is bounded, so a rank that stops ends
+        # the others' next exchange with an error instead of a hang.
+        transport = msf.COMM_HOST if os.environ.get("MSF_COMM") == "host" else msf.COMM_NCCL
+        rdv = "%s:%d" % (os.environ.get("MASTER_ADDR", "127.0.0.1"),
+                         int(os.environ.get("MASTER_PORT", "29500")) + 1)
+        comm = msf.Comm(rank, world, rdv, transport, device=local, timeout_s=180)
 
     work = Path(tempfile.mkdtemp(prefix="msf_bench_r%d_" % rank))
     spec_path = work / "c2.data"
@@ -549,15 +590,16 @@ def main():
         tuning["seconds"] = round(time.time() - t0, 3)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        if comm is not None:
+            comm.allgather(np.zeros(1))
+
+    def max_over_ranks(x):
+        return float(comm.allgather(np.array([x])).max()) if comm is not None else x
 
     if world > 1:
         # weak scaling: one raster of (64 N) x 64 probes (x spacing / N); each
         # rank runs its contiguous 4,096 probes, then the per-probe rows and
         # pixel sums are exchanged and every rank finishes the FEM statistics
-        import shards
-        import torch
         n_x = job.raster.n_x * world
         xp_w = np.arange(n_x) * (job.grid.xperiod / n_x)
         yp_w = np.array(job.raster.y_p[:job.raster.n_y])
@@ -566,24 +608,10 @@ def main():
 
         def step():
             # device time of this rank's probes (msf's own events on its
-            # stream) + device time of the exchange (events on the stream the
-            # collectives run on; host clock with gloo) + the host finish
-            part = shards.run_shard(ctx, spec, job.optics, raster_w, job.detect, rank, world)
-            t_x = time.perf_counter()
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record()
-            amp, inten, acc_a, acc_i = shards.exchange(part, raster_w.n_x * raster_w.n_y, world,
-                                                       dist, coll_dev,
-                                                       job.grid.nx * job.grid.ny)
-            ev1.record()
-            torch.cuda.synchronize()
-            t_x = (1e-3 * ev0.elapsed_time(ev1) if coll_dev == "cuda"
-                   else time.perf_counter() - t_x)
-            t_f = time.perf_counter()
-            res = msf.finish(spec.grid, job.optics, raster_w, job.detect, amp, inten, acc_a,
-                             acc_i)
-            t_f = time.perf_counter() - t_f
-            return res, part, part["seconds_raster"] + t_x + t_f
+            # stream) + the exchange + the host finish (wall clock)
+            res = ctx.run_sharded(spec, job.optics, raster_w, job.detect, comm)
+            sh = res.shard
+            return res, res.seconds_raster + sh["seconds_exchange"] + sh["seconds_finish"]
     for _ in range(args.warmup):
         if world > 1:
             step()
@@ -595,10 +623,10 @@ def main():
         wall0 = time.time()
         for _ in range(args.steps):
             if world > 1:
-                r, part, t_step = step()
+                r, t_step = step()
                 dev_times.append(t_step)
-                launches += part.get("kernel_launches", 0)
-                ps += part["probe_slices"]
+                launches += r.kernel_launches
+                ps += r.probe_slices
             else:
                 r = ctx.run(spec, job.optics, job.raster, job.detect)
                 dev_times.append(r.seconds_raster)
@@ -608,12 +636,7 @@ def main():
             last = r
         wall = time.time() - wall0
     barrier()
-    total_dev = sum(dev_times)
-    if dist is not None:
-        import torch
-        t = torch.tensor([total_dev], device=coll_dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_dev = float(t.item())
+    total_dev = max_over_ranks(sum(dev_times))
     value = ps * world / total_dev  # ps: this rank's probe*slices (equal shards)
     ms_per_step = 1e3 * total_dev / args.steps
 
@@ -677,9 +700,8 @@ def main():
         for _ in range(e2e_steps):
             s2 = ctx.specimen(job.grid, q, z)
             if world > 1:
-                _, p2 = shards.run_sharded(ctx, s2, job.optics, raster_w, job.detect, rank,
-                                           world, dist, device=coll_dev)
-                e2e_ps += p2["probe_slices"]
+                r2 = ctx.run_sharded(s2, job.optics, raster_w, job.detect, comm)
+                e2e_ps += r2.probe_slices
             else:
                 r2 = ctx.run(s2, job.optics, job.raster, job.detect)
                 e2e_ps += r2.probe_slices
@@ -691,11 +713,8 @@ def main():
                "h2d_bytes_per_step": int(h2d / e2e_steps),
                "d2h_bytes_per_step": int(d2h / e2e_steps),
                "includes": "atom upload, LUT/slicing/transmission build, raster, result copy"}
-        if dist is not None:
-            import torch
-            t = torch.tensor([e2e_t], device=coll_dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e["value"] = e2e_ps * world / float(t.item())
+        if comm is not None:
+            e2e["value"] = e2e_ps * world / max_over_ranks(e2e_t)
 
     # plain one-probe-at-a-time GPU path and the FP32 outputs' error
     versus = None
@@ -761,8 +780,8 @@ def main():
         print(json.dumps(line))
     spec.close()
     ctx.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    if comm is not None:
+        comm.close()
     return 0
 
 

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MSF_ABI_VERSION 3
+#define MSF_ABI_VERSION 4
 
 typedef enum {
   MSF_OK = 0,
@@ -195,6 +195,14 @@ msf_status msf_specimen_transmission(const msf_specimen* spec, int32_t slice,
                                      double* out);
 /* Bytes of device memory the specimen holds. */
 int64_t msf_specimen_device_bytes(const msf_specimen* spec);
+/* --paptif (slice.cpp:1660-1690): specimens built by `ctx` after
+ * msf_context_keep_potentials(ctx, 1) keep a host copy of every slice's
+ * projected potential sigma*V before the exponential (the sum of the
+ * scatterers' shifted lookup tables); msf_specimen_potential copies slice
+ * `slice`'s 2*nx*ny doubles ([x][y] complex) into `out`, MSF_ERR_ARG when
+ * the specimen was built without them. */
+msf_status msf_context_keep_potentials(msf_context* ctx, int32_t on);
+msf_status msf_specimen_potential(const msf_specimen* spec, int32_t slice, double* out);
 /* Columns (ky values) in which the band limit keeps any kx (bw_limit.cpp:
  * 30-47 with the transmission cut-off); the slice passes move no data for
  * the others, which only ever hold zeros between the passes. */
@@ -241,8 +249,8 @@ typedef struct {
   int32_t pipe;               /* slice-pass variants: bit 0 pipelined column
                                  pass, bit 1 pipelined row pass, bit 2 row
                                  pass with staged slice tables (FP32), bit 3
-                                 that row pass's alternative FFT radix
-                                 schedule                                    */
+                                 the FP32 split-wave row pass on its
+                                 alternative FFT radix schedule             */
   double ns_per_probe_slice;  /* measured time of the two slice passes        */
 } msf_tuning;
 /* Times the two slice passes of `spec`'s grid (CUDA events, after a
@@ -308,6 +316,51 @@ msf_status msf_finish(const msf_grid* grid, const msf_optics* optics,
                       const double* inten, const double* acc_a, const double* acc_i,
                       msf_results* results);
 
+/* ---- one raster over several ranks (the reference's mpirun -np K,
+ * tem.cpp:90; probe shares adfstem.cpp:1556-1606; collective sums
+ * adfstem.cpp:2256, 2489-2782) ------------------------------------------- */
+typedef struct msf_comm msf_comm;
+#define MSF_COMM_NCCL 1 /* exchange on device buffers through NCCL (one GPU per rank) */
+#define MSF_COMM_HOST 2 /* exchange through the TCP bootstrap (ranks may share a GPU) */
+/* Joins `world` ranks (one process each).  Rank 0 listens at `rendezvous`
+ * ("host:port", e.g. torchrun's MASTER_ADDR:MASTER_PORT; unused when
+ * world == 1), the others connect to it; with MSF_COMM_NCCL every rank then
+ * creates an NCCL communicator on `device` (libnccl.so.2 is loaded at this
+ * point; MSF_ERR_UNSUPPORTED when it is absent).  Every connection and
+ * exchange waits at most `timeout_s` seconds (<= 0: 60) and then returns
+ * MSF_ERR_TIMEOUT, so a rank that never joins or stops answering surfaces
+ * as an error on the others.  Collective: every rank calls it. */
+msf_status msf_comm_create(int32_t rank, int32_t world, const char* rendezvous,
+                           int32_t transport, int32_t device, double timeout_s,
+                           msf_comm** out);
+void msf_comm_destroy(msf_comm* comm);
+/* Host all-gather over the bootstrap connections: recv[world * bytes] gets
+ * every rank's `bytes` of `send` in rank order.  Collective. */
+msf_status msf_comm_allgather_host(msf_comm* comm, const void* send, int64_t bytes,
+                                   void* recv);
+typedef struct {
+  int64_t p_begin, p_end;    /* out: this rank's probes (raster order)        */
+  double seconds_shard;      /* out: wall time of this rank's probes           */
+  double seconds_exchange;   /* out: wall time of the exchange                 */
+  double seconds_finish;     /* out: wall time of the host finish              */
+} msf_shard_info;
+/* msf_run over the communicator's ranks: each rank runs a contiguous share
+ * of the probes (sizes differ by at most one, lower ranks first), then one
+ * exchange step all-gathers the per-probe detector rows and the per-pixel
+ * sums of the FEM pixel modes (added in rank order on every rank), and
+ * every rank finishes the same ADF image, FEM statistics and correlograph
+ * into `results`; first_psi is filled on rank 0 and final_psi (the last
+ * probe's exit wave, sent on from the rank that ran it) on every rank.
+ * probe_slices,
+ * kernel_launches, seconds_raster and the pass times describe this rank's
+ * share.  With world == 1 the outputs equal msf_run's bit for bit.
+ * Collective: every rank calls it with the same raster, detector and set
+ * of output buffers; `info` may be NULL. */
+msf_status msf_run_sharded(msf_context* ctx, const msf_specimen* spec,
+                           const msf_optics* optics, const msf_raster* raster,
+                           const msf_detect* detect, msf_comm* comm, msf_results* results,
+                           msf_shard_info* info);
+
 /* ---- slot batches and serving (no counterpart in the reference) -------- */
 /* Several rasters at once: results[i] is what msf_run(ctx, specs[i],
  * &optics[i], &rasters[i], &detects[i], &results[i]) returns, within FP32
@@ -344,11 +397,15 @@ typedef struct {
 
 typedef struct msf_server msf_server;
 /* A request loop on one GPU (FP32 wavefields).  A worker thread admits
- * requests in arrival order while their estimated device bytes fit
- * `opt->hbm_budget` (0: 80 % of free memory), builds each specimen, and
+ * requests in arrival order whose estimated device bytes fit
+ * `opt->hbm_budget` (0: 80 % of free memory; a request that does not fit
+ * lets later ones past it for 5 s, then holds them back until it fits),
+ * builds each specimen (smallest first, unless one has waited 5 s), and
  * feeds its probes into the slot lane of its grid size (`slots` wavefields
  * per lane; 0: about 2 GiB of wavefields, 16..256, by grid size); requests
- * that arrive while others run join the running launches as slots free up. */
+ * that arrive while others run join the running launches as slots free up,
+ * a lane shares its slots fairly among its rasters, and lanes of smaller
+ * grids run on higher-priority streams. */
 msf_status msf_server_create(const msf_options* opt, int32_t slots, msf_server** out);
 /* Queue a request; returns at once with its ticket. */
 msf_status msf_server_submit(msf_server* srv, const msf_request* req, uint64_t* ticket);
@@ -359,6 +416,15 @@ msf_status msf_server_submit(msf_server* srv, const msf_request* req, uint64_t* 
 msf_status msf_server_poll(msf_server* srv, uint64_t ticket, int32_t wait_ms,
                            msf_results* results);
 msf_status msf_server_stats_get(msf_server* srv, msf_server_stats* out);
+/* Latency of the completed requests per grid size (submission to
+ * completion, as msf_server_stats): fills up to `cap` entries in order of
+ * grid size and returns how many grid sizes have completed requests. */
+typedef struct {
+  int32_t nx, ny;
+  int64_t completed;
+  double p50_s, p99_s, max_s;
+} msf_server_grid_stats;
+int32_t msf_server_grid_stats_get(msf_server* srv, msf_server_grid_stats* out, int32_t cap);
 /* Cancels a request: one still waiting for admission is dropped at once;
  * one already admitted runs to the end of its probes (they share launches
  * with other requests) and its results are discarded; a finished one not

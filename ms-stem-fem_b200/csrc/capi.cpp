@@ -236,6 +236,27 @@ msf_status msf_run_plain(msf_context* ctx, const msf_specimen* spec, const msf_o
   return run_raster_plain(ctx, spec, optics, raster, detect, results);
 }
 
+msf_status msf_context_keep_potentials(msf_context* ctx, int32_t on) {
+  if (!ctx) return MSF_ERR_ARG;
+  ctx->keep_potentials = on != 0;
+  return MSF_OK;
+}
+
+msf_status msf_specimen_potential(const msf_specimen* spec, int32_t slice, double* out) {
+  if (!spec || !out || slice < 0 || slice >= spec->n_slices) {
+    set_error("msf_specimen_potential: no such slice");
+    return MSF_ERR_ARG;
+  }
+  const size_t plane = (size_t)spec->g.nx * spec->g.ny;
+  if (spec->h_potential.size() < 2 * plane * (size_t)(slice + 1)) {
+    set_error("msf_specimen_potential: the specimen was built without "
+              "msf_context_keep_potentials");
+    return MSF_ERR_ARG;
+  }
+  std::memcpy(out, spec->h_potential.data() + 2 * plane * slice, 16 * plane);
+  return MSF_OK;
+}
+
 int32_t msf_segment_count(const msf_grid* grid, const msf_detect* detect) {
   if (!grid || !detect) return -1;
   if (!(detect->outputs & MSF_OUT_FEM_MASK)) return 1;

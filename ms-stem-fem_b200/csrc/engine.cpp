@@ -202,6 +202,19 @@ constexpr int64_t kPotentialFftAtoms = 64;
 
 }  // namespace
 
+// Copies slice s's projected potential (before the exponential, as the
+// reference's --paptif images show it, slice.cpp:1660-1690) to the
+// specimen's host table.
+msf_status keep_potential(msf_context* ctx, msf_specimen* spec, const double* t64, int64_t s) {
+  const int64_t plane = (int64_t)spec->g.nx * spec->g.ny;
+  if ((int64_t)spec->h_potential.size() < 2 * plane * (s + 1))
+    spec->h_potential.resize((size_t)(2 * plane * (s + 1)));
+  MSF_CUDA(cudaMemcpyAsync(spec->h_potential.data() + 2 * plane * s, t64, 16 * plane,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  MSF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MSF_OK;
+}
+
 msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms* atoms,
                           msf_specimen* spec) {
   TraceScope trace_scope("specimen_build");
@@ -406,12 +419,22 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
       MSF_CUDA(launch_histogram_lut(t64, hist.as<double>(), luts_k.as<double>(),
                                     (int)species.size(), plane, ctx->stream));
       MSF_TRY(fft2d_f64(ctx, g, t64, 1, true, 1.0));
-      MSF_CUDA(launch_transmission_exp(t64, plane, 1.0 / std::sqrt((double)(g.nx * (int64_t)g.ny)),
-                                       ctx->stream));
+      const double sc = 1.0 / std::sqrt((double)(g.nx * (int64_t)g.ny));
+      if (ctx->keep_potentials) {  // scale first, keep, exponentiate (same values)
+        MSF_CUDA(launch_scale(t64, plane, sc, nullptr, ctx->stream));
+        MSF_TRY(keep_potential(ctx, spec, t64, s));
+        MSF_CUDA(launch_transmission_exp(t64, plane, 1.0, ctx->stream));
+      } else {
+        MSF_CUDA(launch_transmission_exp(t64, plane, sc, ctx->stream));
+      }
     } else {
       MSF_CUDA(launch_potential(t64, luts.as<double>(), g.nx, g.ny, dsx.as<int32_t>() + s0,
                                 dsy.as<int32_t>() + s0, dsp.as<int32_t>() + s0, (int)cnt,
-                                ctx->stream));
+                                ctx->stream, !ctx->keep_potentials));
+      if (ctx->keep_potentials) {
+        MSF_TRY(keep_potential(ctx, spec, t64, s));
+        MSF_CUDA(launch_transmission_exp(t64, plane, 1.0, ctx->stream));
+      }
     }
     a.psi = t64;
     MSF_TRY(ctx->twiddles(g.ny, true, &a.tw));
@@ -513,9 +536,9 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   // the same kernels run_raster launches for slices after the first
   const int pipe = ctx->pipe_for(g.nx, g.ny);
   const bool staged_row = !fp64 && staged_row_supported(g.nx, g.ny) && (pipe & MSF_ROW_STAGED);
-  const int row_sched = staged_row && (pipe & MSF_ROW_ALT) ? 1 : 0;
-  const bool pipe_row =
-      !fp64 && !staged_row && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
+  const int row_sched = !fp64 && staged_row_supported(g.nx, g.ny) && (pipe & MSF_ROW_ALT) ? 1 : 0;
+  const bool pipe_row = !fp64 && !staged_row && !row_sched && pipe_supported(g.nx, g.ny) &&
+                        (pipe & MSF_PIPE_ROW);
   const bool pipe_col = pipe_supported(g.nx, g.ny, fp64) && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
@@ -531,10 +554,11 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
   PassArgs row_staged = row;  // schedule 1 reads the zero bits in its own layout
   if (row_sched == 1 && row.row_dead_bits) row_staged.row_dead_bits = spec->dead_bits_alt.as<uint32_t>();
   auto row_pass = [&]() {
-    return staged_row ? launch_row_split_staged(row_staged, d_err.as<int>(), ctx->stream,
-                                                row_sched)
-           : pipe_row ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
-                      : launch_row(fp64, rop, row, ctx->stream);
+    return staged_row       ? launch_row_split_staged(row_staged, d_err.as<int>(), ctx->stream,
+                                                      row_sched)
+           : row_sched == 1 ? launch_row_split_alt(row_staged, ctx->stream)
+           : pipe_row       ? launch_row_split_pipe(row, d_err.as<int>(), ctx->stream)
+                            : launch_row(fp64, rop, row, ctx->stream);
   };
   auto col_pass = [&]() {
     return pipe_col ? launch_col_slice_pipe(col, false, col_map, d_err.as<int>(), ctx->stream, fp64)
@@ -1041,9 +1065,9 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   // persistent TMA-pipelined passes for FP32 grids they support
   const int pipe = ctx->pipe_for(g.nx, g.ny);
   const bool staged_row = !fp64 && staged_row_supported(g.nx, g.ny) && (pipe & MSF_ROW_STAGED);
-  const int row_sched = staged_row && (pipe & MSF_ROW_ALT) ? 1 : 0;
-  const bool pipe_row =
-      !fp64 && !staged_row && pipe_supported(g.nx, g.ny) && (pipe & MSF_PIPE_ROW);
+  const int row_sched = !fp64 && staged_row_supported(g.nx, g.ny) && (pipe & MSF_ROW_ALT) ? 1 : 0;
+  const bool pipe_row = !fp64 && !staged_row && !row_sched && pipe_supported(g.nx, g.ny) &&
+                        (pipe & MSF_PIPE_ROW);
   const bool pipe_col = pipe_supported(g.nx, g.ny, fp64) && (pipe & MSF_PIPE_COL);
   alignas(64) unsigned char col_map[128];
   DevBuf d_err;
@@ -1101,10 +1125,13 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
         op = s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT;
         row.psi0 = P.psi0_tab.as<float>() + 2 * plane * s;
       }
-      if (staged_row && op == ROW_SPLIT) {
+      if ((staged_row || row_sched == 1) && op == ROW_SPLIT) {
         PassArgs rs = row;  // schedule 1 reads the zero bits in its own layout
         if (row_sched == 1 && rs.row_dead_bits) rs.row_dead_bits = spec->dead_bits_alt.as<uint32_t>();
-        MSF_CUDA(launch_row_split_staged(rs, d_err.as<int>(), ctx->stream, row_sched));
+        if (staged_row)
+          MSF_CUDA(launch_row_split_staged(rs, d_err.as<int>(), ctx->stream, row_sched));
+        else
+          MSF_CUDA(launch_row_split_alt(rs, ctx->stream));
       }
       else if (pipe_row && op == ROW_SPLIT)
         MSF_CUDA(launch_row_split_pipe(row, d_err.as<int>(), ctx->stream));

@@ -70,7 +70,8 @@ struct DevBuf {
 // with its transmission and vacuum rows staged in shared memory by bulk
 // copies (which takes precedence over MSF_PIPE_ROW).
 constexpr int MSF_PIPE_COL = 1, MSF_PIPE_ROW = 2, MSF_ROW_STAGED = 4;
-// with MSF_ROW_STAGED: the row pass's alternative FFT radix schedule
+// the split-wave row pass's alternative FFT radix schedule (16 elements a
+// thread; staged or plain)
 constexpr int MSF_ROW_ALT = 8;
 constexpr int MSF_PIPE_ALL = MSF_PIPE_COL | MSF_PIPE_ROW | MSF_ROW_STAGED | MSF_ROW_ALT;
 
@@ -109,6 +110,9 @@ struct msf_context {
     return (pipe_env || it == tuned.end()) ? pipe : it->second.pipe;
   }
   bool pipe_env = false;  // MSF_PIPE given: it wins over tuning
+  // specimens built by this context keep a host copy of every slice's
+  // projected potential before the exponential (msf_specimen_potential)
+  bool keep_potentials = false;
   msf_status alloc(msf::DevBuf* b, size_t bytes);
   msf_status twiddles(int n, bool fp64, const void** out);
 };
@@ -133,6 +137,7 @@ struct msf_specimen {
   int n_live_groups = 0, n_live_columns = 0;
   msf::DevBuf kx, ky;         // FP64 domains for device set-up kernels
   std::vector<double> hprop;  // FP64 propagators, host copy
+  std::vector<double> h_potential;  // [slice][nx][ny] complex, when kept
   double seconds_setup = 0;
   int64_t device_bytes = 0;
 };

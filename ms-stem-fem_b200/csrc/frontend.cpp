@@ -985,7 +985,7 @@ struct RunBuffers {
 // otherwise the launch tiling is measured (msf_tune) and the file written.
 // Skipped when --batch fixes the tiling.
 void apply_wisdom(const msf_grid& grid, msf_context* ctx, const msf_specimen* spec,
-                  const msf_options& o) {
+                  const msf_options& o, bool write_file = true) {
   if (o.batch > 0) return;
   const std::string name = "msf_wisdom_" + std::to_string(grid.nx) + "x" +
                            std::to_string(grid.ny) + (o.precision == MSF_FP32 ? "_fp32" : "_fp64");
@@ -1001,6 +1001,7 @@ void apply_wisdom(const msf_grid& grid, msf_context* ctx, const msf_specimen* sp
   const int64_t len = msf_wisdom_export(ctx, nullptr, 0);
   std::vector<char> buf((size_t)len + 1);
   msf_wisdom_export(ctx, buf.data(), len + 1);
+  if (!write_file) return;
   std::ofstream out(name.c_str());
   out << buf.data();
 }
@@ -1267,6 +1268,147 @@ msf_status msf_write_outputs(const msf_job* j, const msf_results* r) {
   return MSF_OK;
 }
 
+namespace {
+
+// --paptif (slice.cpp:1660-1690 through func.cpp:2024-2362): per slice
+// n = 1, 2, ..., 16-bit images of the projected potential before the
+// exponential: magnitude (linear and log), real part (linear and log) and
+// imaginary part, named <prefix>_pap_slice<n>_1_complex_fftw_operand_*.
+// Each image is min/max scaled over the slice.  The reference starts the
+// imaginary part's running min / max from uninitialised values (its
+// initialisation lines set the real part's twice), so its imaginary images
+// are not defined; here they start from the first sample like the others.
+// As in the reference both imaginary images use the log scaling.
+msf_status write_paptif(const msf_job* j, const msf_specimen* spec) {
+  const size_t nx = j->nx, ny = j->ny, plane = nx * ny;
+  const double xres = nx / (j->xperiod * j->dupe_x * 1e-8);
+  const double yres = ny / (j->yperiod * j->dupe_y * 1e-8);
+  std::vector<double> v(2 * plane), mag(plane), re(plane), im(plane);
+  for (int32_t sl = 0; sl < spec->n_slices; ++sl) {
+    msf_status st = msf_specimen_potential(spec, sl, v.data());
+    if (st != MSF_OK) return st;
+    for (size_t k = 0; k < plane; ++k) {
+      re[k] = v[2 * k];
+      im[k] = v[2 * k + 1];
+      mag[k] = std::sqrt(std::pow(re[k], 2) + std::pow(im[k], 2));
+    }
+    auto range = [&](const std::vector<double>& a, double* mn, double* mx) {
+      *mn = *mx = a[0];
+      for (double x : a) { if (x > *mx) *mx = x; if (x < *mn) *mn = x; }
+    };
+    const std::string base = j->output_prefix + "_pap_slice" + std::to_string(sl + 1) +
+                             "_1_complex_fftw_operand_";
+    double mn, mx;
+    bool ok = true;
+    range(mag, &mn, &mx);
+    ok = ok && write_tif16(base + "mag_output.tif", mag.data(), nx, ny, mn, mx, false, xres, yres, 3);
+    ok = ok && write_tif16(base + "mag_output_logscale.tif", mag.data(), nx, ny, mn, mx, true,
+                           xres, yres, 3);
+    range(re, &mn, &mx);
+    ok = ok && write_tif16(base + "re.tif", re.data(), nx, ny, mn, mx, false, xres, yres, 3);
+    ok = ok && write_tif16(base + "re_logscale.tif", re.data(), nx, ny, mn, mx, true, xres, yres, 3);
+    range(im, &mn, &mx);
+    ok = ok && write_tif16(base + "im.tif", im.data(), nx, ny, mn, mx, true, xres, yres, 3);
+    ok = ok && write_tif16(base + "im_logscale.tif", im.data(), nx, ny, mn, mx, true, xres, yres, 3);
+    if (!ok) {
+      msf::set_error("could not write " + base + "*.tif");
+      return MSF_ERR_IO;
+    }
+  }
+  return MSF_OK;
+}
+
+// One raster over `world` processes (one per GPU): every rank builds the
+// specimen, runs its share of the probes and joins the exchange; rank 0
+// alone writes the output files, as the reference's root rank does.  The
+// rendezvous is MSF_RENDEZVOUS (host:port), else MASTER_ADDR with the port
+// after MASTER_PORT (torchrun's own store listens on MASTER_PORT); the
+// transport MSF_COMM = nccl (default; one GPU per rank) or host (ranks may
+// share a GPU); the device is the local rank modulo the GPUs present.
+int32_t sharded_main(msf_job* j, msf_options o, int rank, int world, int local) {
+  std::string rdv;
+  if (const char* r = std::getenv("MSF_RENDEZVOUS")) rdv = r;
+  const char* ma = std::getenv("MASTER_ADDR");
+  const char* mp = std::getenv("MASTER_PORT");
+  if (rdv.empty() && ma && mp) rdv = std::string(ma) + ":" + std::to_string(std::atoi(mp) + 1);
+  const char* tr = std::getenv("MSF_COMM");
+  const int transport = (tr && std::string(tr) == "host") ? MSF_COMM_HOST : MSF_COMM_NCCL;
+  double timeout_s = 300.0;
+  if (const char* t = std::getenv("MSF_COMM_TIMEOUT")) timeout_s = std::atof(t);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) ndev = 1;
+  o.device = local % ndev;
+  msf_comm* comm = nullptr;
+  msf_context* ctx = nullptr;
+  msf_specimen* spec = nullptr;
+  msf_grid grid;
+  msf_atoms atoms;
+  msf_optics optics;
+  msf_raster raster;
+  msf_detect det;
+  msf_job_describe(j, &grid, &atoms, &optics, &raster, &det);
+  int rc = 1;
+  msf_status st = MSF_OK;
+  if (rdv.empty()) {
+    msf::set_error("a run over " + std::to_string(world) + " ranks needs MSF_RENDEZVOUS=host:port "
+                   "or MASTER_ADDR and MASTER_PORT");
+    st = MSF_ERR_ARG;
+  } else if ((st = msf_context_create(&o, &ctx)) == MSF_OK &&
+             (st = msf_context_keep_potentials(ctx, rank == 0 && j->flags.pap_tif)) == MSF_OK &&
+             (st = msf_comm_create(rank, world, rdv.c_str(), transport, o.device, timeout_s,
+                                   &comm)) == MSF_OK &&
+             (st = msf_specimen_create(ctx, &grid, &atoms, &spec)) == MSF_OK &&
+             (rank != 0 || !j->flags.pap_tif || (st = write_paptif(j, spec)) == MSF_OK)) {
+    apply_wisdom(grid, ctx, spec, o, rank == 0);  // one writer of the wisdom file
+    RunBuffers b;
+    b.setup(j, grid, raster, det, true);
+    if ((st = msf_run_sharded(ctx, spec, &optics, &raster, &det, comm, &b.r, nullptr)) ==
+            MSF_OK &&
+        (rank != 0 || (st = msf_write_outputs(j, &b.r)) == MSF_OK))
+      rc = 0;
+  }
+  if (rc != 0) std::cerr << "ms-stem-fem (rank " << rank << "): " << msf::last_error() << std::endl;
+  msf_comm_destroy(comm);
+  msf_specimen_destroy(spec);
+  msf_context_destroy(ctx);
+  msf_job_destroy(j);
+  return rc;
+}
+
+// Ranks of a multi-process launch, as `mpirun -np K` gives the reference
+// (tem.cpp:90): torchrun's RANK / WORLD_SIZE / LOCAL_RANK, Open MPI's
+// OMPI_COMM_WORLD_*, MPICH's PMI_RANK / PMI_SIZE, or Slurm's SLURM_PROCID /
+// SLURM_NTASKS / SLURM_LOCALID.  world 1 when none is set.
+struct Launch {
+  int rank = 0, world = 1, local = 0;
+};
+Launch launch_from_env() {
+  auto num = [](const char* name, int* out) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return false;
+    *out = std::atoi(v);
+    return true;
+  };
+  Launch l;
+  const char* sets[][3] = {{"WORLD_SIZE", "RANK", "LOCAL_RANK"},
+                           {"OMPI_COMM_WORLD_SIZE", "OMPI_COMM_WORLD_RANK",
+                            "OMPI_COMM_WORLD_LOCAL_RANK"},
+                           {"PMI_SIZE", "PMI_RANK", "MPI_LOCALRANKID"},
+                           {"SLURM_NTASKS", "SLURM_PROCID", "SLURM_LOCALID"}};
+  for (auto& s : sets) {
+    int w = 0, r = 0;
+    if (num(s[0], &w) && w > 1 && num(s[1], &r)) {
+      l.world = w;
+      l.rank = r;
+      if (!num(s[2], &l.local)) l.local = r;
+      break;
+    }
+  }
+  return l;
+}
+
+}  // namespace
+
 int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) {
   msf_job* j = nullptr;
   msf_status st = msf_parse_cmdline(argc, argv, &j);
@@ -1278,6 +1420,8 @@ int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) 
   o.precision = MSF_FP64;
   o.use_graphs = 1;
   if (opt) o = *opt;
+  const Launch launch = launch_from_env();
+  if (launch.world > 1) return sharded_main(j, o, launch.rank, launch.world, launch.local);
   msf_context* ctx = nullptr;
   msf_specimen* spec = nullptr;
   msf_grid grid;
@@ -1288,7 +1432,9 @@ int32_t msf_main(int32_t argc, const char* const* argv, const msf_options* opt) 
   msf_job_describe(j, &grid, &atoms, &optics, &raster, &det);
   int rc = 1;
   if ((st = msf_context_create(&o, &ctx)) == MSF_OK &&
-      (st = msf_specimen_create(ctx, &grid, &atoms, &spec)) == MSF_OK) {
+      (st = msf_context_keep_potentials(ctx, j->flags.pap_tif)) == MSF_OK &&
+      (st = msf_specimen_create(ctx, &grid, &atoms, &spec)) == MSF_OK &&
+      (!j->flags.pap_tif || (st = write_paptif(j, spec)) == MSF_OK)) {
     apply_wisdom(grid, ctx, spec, o);
     RunBuffers b;
     b.setup(j, grid, raster, det, true);

@@ -16,6 +16,7 @@
 #include "kernels.h"
 #include "fft_core.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -59,19 +60,26 @@ constexpr int kSmemBudget = 220 * 1024;
 #ifndef MSF_THREADS_PER_SM_F64
 #define MSF_THREADS_PER_SM_F64 256
 #endif
-constexpr int min_blocks(int real_bytes, int threads, int n) {
+// FP32 row passes on the alternative FFT schedule (16 or 8 elements a
+// thread): 512 threads per SM (at most 128 registers; 640 spilled heavily).
+#ifndef MSF_THREADS_PER_SM_ALT
+#define MSF_THREADS_PER_SM_ALT 512
+#endif
+constexpr int min_blocks(int real_bytes, int threads, int n, int schedule = 0) {
   if (real_bytes == 8)
     return MSF_THREADS_PER_SM_F64 > threads ? MSF_THREADS_PER_SM_F64 / threads : 1;
-  const int want = n >= 2048 ? MSF_THREADS_PER_SM_LONG : MSF_THREADS_PER_SM;
+  const int want = schedule == 1 ? MSF_THREADS_PER_SM_ALT
+                   : n >= 2048   ? MSF_THREADS_PER_SM_LONG
+                                 : MSF_THREADS_PER_SM;
   return threads >= want ? 1 : want / threads;
 }
 
 // Lines (rows) per CTA of a row pass: about MSF_ROW_THREADS (FP64) or
 // MSF_ROW_THREADS_F32 threads, small CTAs so that several reside per SM and
 // their load / FFT / store phases overlap.
-template <typename Real, int N>
+template <typename Real, int N, int V = 0>
 constexpr int row_lines() {
-  using Sh = Shape<N, Real>;
+  using Sh = Shape<N, Real, V>;
   constexpr int bytes = (Sh::N + (Sh::N >> ilog2(Sh::R0)) + 16) * (int)sizeof(Cx<Real>);
   int l = (sizeof(Real) == 4 ? MSF_ROW_THREADS_F32 : MSF_ROW_THREADS) / Sh::T;
   if (l < 1) l = 1;
@@ -113,12 +121,13 @@ __device__ __forceinline__ void split_update(C (&v)[Sh::E], const C* __restrict_
   }
 }
 
-template <typename Real, int N, int LINES, int OP>
-__global__ void __launch_bounds__(LINES * Shape<N, Real>::T,
-                                  min_blocks((int)sizeof(Real), LINES * Shape<N, Real>::T, N))
+template <typename Real, int N, int LINES, int OP, int V = 0>
+__global__ void __launch_bounds__(LINES * Shape<N, Real, V>::T,
+                                  min_blocks((int)sizeof(Real), LINES * Shape<N, Real, V>::T, N,
+                                             V))
 row_kernel(const PassArgs a) {
   using C = Cx<Real>;
-  using Sh = Shape<N, Real>;
+  using Sh = Shape<N, Real, V>;
   using SM = Smem<Sh, (int)sizeof(Cx<Real>), LINES, false>;
   constexpr int E = Sh::E, T = Sh::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -321,13 +330,13 @@ col_kernel(const PassArgs a) {
   for (int m = 0; m < E; ++m) col[(int64_t)(t + T * m) * ny] = v[m];
 }
 
-template <typename Real, int N, int OP>
+template <typename Real, int N, int OP, int V = 0>
 cudaError_t row_launch(const PassArgs& a, cudaStream_t s) {
-  constexpr int L = row_lines<Real, N>();
-  using Sh = Shape<N, Real>;
+  constexpr int L = row_lines<Real, N, V>();
+  using Sh = Shape<N, Real, V>;
   constexpr int smem = L * Smem<Sh, (int)sizeof(Cx<Real>), L, false>::stride * (int)sizeof(Cx<Real>);
   static PerDevice configured;
-  auto k = row_kernel<Real, N, L, OP>;
+  auto k = row_kernel<Real, N, L, OP, V>;
   if (cudaError_t e = smem_limit_once((const void*)k, smem, configured); e != cudaSuccess)
     return e;
   if (a.nx % L != 0) return cudaErrorInvalidValue;
@@ -424,6 +433,7 @@ constexpr int kPotChunk = 512;
 // memory in chunks), in the reference's atom order so the FP64 sums equal
 // slice.cpp:1594-1649 term for term.  The LUT spans the whole cell, so every
 // atom contributes to every tile; no global atomics are used.
+template <bool EXP>
 __global__ void potential_kernel(double2* __restrict__ t, const double2* __restrict__ luts,
                                  int nx, int ny, const int32_t* __restrict__ asx,
                                  const int32_t* __restrict__ asy,
@@ -460,11 +470,14 @@ __global__ void potential_kernel(double2* __restrict__ t, const double2* __restr
   if (j < ny) {
 #pragma unroll
     for (int r = 0; r < kPotRows; ++r) {
-      // slice.cpp:1700-1725
-      const double e = exp(-(acc[r].y));
-      double sn, cs;
-      sincos(acc[r].x, &sn, &cs);
-      t[(int64_t)(i0 + r) * ny + j] = make_double2(e * cs, e * sn);
+      if constexpr (EXP) {  // slice.cpp:1700-1725
+        const double e = exp(-(acc[r].y));
+        double sn, cs;
+        sincos(acc[r].x, &sn, &cs);
+        t[(int64_t)(i0 + r) * ny + j] = make_double2(e * cs, e * sn);
+      } else {  // the projected potential itself (what --paptif shows)
+        t[(int64_t)(i0 + r) * ny + j] = acc[r];
+      }
     }
   }
 }
@@ -941,6 +954,16 @@ cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_row_split_alt(const PassArgs& a, cudaStream_t s) {
+  switch (a.ny) {
+    case 256: return row_launch<float, 256, ROW_SPLIT, 1>(a, s);
+    case 512: return row_launch<float, 512, ROW_SPLIT, 1>(a, s);
+    case 1024: return row_launch<float, 1024, ROW_SPLIT, 1>(a, s);
+    case 2048: return row_launch<float, 2048, ROW_SPLIT, 1>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s) {
   if (fp64) {
     switch (op) {
@@ -982,13 +1005,18 @@ cudaError_t launch_lut_synth(double* out, const double* kx, const double* ky, in
 
 cudaError_t launch_potential(double* t, const double* luts, int nx, int ny,
                              const int32_t* asx, const int32_t* asy, const int32_t* asp,
-                             int n_atoms, cudaStream_t s) {
+                             int n_atoms, cudaStream_t s, bool exponentiate) {
   if (nx % kPotRows) return cudaErrorInvalidValue;
   const int tpb = ny < 256 ? ny : 256;
   dim3 grid((ny + tpb - 1) / tpb, nx / kPotRows);
-  potential_kernel<<<grid, tpb, 0, s>>>(reinterpret_cast<double2*>(t),
-                                        reinterpret_cast<const double2*>(luts), nx, ny,
-                                        asx, asy, asp, n_atoms);
+  if (exponentiate)
+    potential_kernel<true><<<grid, tpb, 0, s>>>(reinterpret_cast<double2*>(t),
+                                                reinterpret_cast<const double2*>(luts), nx, ny,
+                                                asx, asy, asp, n_atoms);
+  else
+    potential_kernel<false><<<grid, tpb, 0, s>>>(reinterpret_cast<double2*>(t),
+                                                 reinterpret_cast<const double2*>(luts), nx,
+                                                 ny, asx, asy, asp, n_atoms);
   return cudaGetLastError();
 }
 
@@ -1111,6 +1139,25 @@ cudaError_t launch_propagate(double* psi, const double* px, const double* py, co
   propagate_kernel<<<blocks_for((int64_t)nx * ny, 256), 256, 0, s>>>(
       reinterpret_cast<double2*>(psi), reinterpret_cast<const double2*>(px),
       reinterpret_cast<const double2*>(py), lo, hi, nx, ny);
+  return cudaGetLastError();
+}
+
+// out[p] = in[0][p] + in[1][p] + ... in rank order (FP64, no contraction)
+__global__ void rank_sum_kernel(const double* __restrict__ in, int world, int64_t n,
+                                double* __restrict__ out) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int r = 0; r < world; ++r) acc = __dadd_rn(acc, in[(int64_t)r * n + p]);
+    out[p] = acc;
+  }
+}
+
+cudaError_t launch_rank_sum(const double* in, int world, int64_t n, double* out,
+                            cudaStream_t s) {
+  if (world <= 0 || n <= 0) return cudaErrorInvalidValue;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 8 * (int64_t)sm_count());
+  rank_sum_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, world, n, out);
   return cudaGetLastError();
 }
 

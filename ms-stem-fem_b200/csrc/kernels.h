@@ -139,6 +139,11 @@ int row_line_threads(int n, bool fp64);
 // Columns per tile of the pipelined column pass (0 if unsupported).
 int pipe_cols_for(int nx, bool fp64);
 cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s);
+// The FP32 split-wave row pass (ROW_SPLIT) on the alternative FFT radix
+// schedule (16 elements a thread from 512 points, 8 at 256; row_dead_bits
+// in that schedule's layout, staged_row_threads(ny, 1)); row lengths
+// 256..2048.
+cudaError_t launch_row_split_alt(const PassArgs& a, cudaStream_t s);
 cudaError_t launch_col(bool fp64, ColOp op, const PassArgs& a, cudaStream_t s);
 
 // ---- persistent TMA-pipelined slice passes (kernels_pipe.cu) ----
@@ -183,10 +188,11 @@ cudaError_t launch_lut_synth(double* out, const double* kx, const double* ky,
                              double ymin, cudaStream_t s);
 // t(x,y) = sum of shifted LUTs over the slice's atoms, then
 // e^{-Im} (cos Re, sin Re) (slice.cpp:1544-1725).  Atoms in slice order.
+// exponentiate = false: stop at the sum (the projected potential).
 cudaError_t launch_potential(double* t, const double* luts, int nx, int ny,
                              const int32_t* atom_sx, const int32_t* atom_sy,
                              const int32_t* atom_species, int n_atoms,
-                             cudaStream_t s);
+                             cudaStream_t s, bool exponentiate = true);
 // Potential by FFT convolution (the direct sum's exact equivalent):
 // H[sp[k]][pix[k]] = count[k] on zeroed planes; out = sum_s H_s * lut_s in
 // k-space; t = e^{-Im v} (cos Re v, sin Re v) with v = t * scale.
@@ -277,6 +283,10 @@ cudaError_t launch_mtf_magnitude(bool fp64, const void* psi, int64_t stride, int
 cudaError_t launch_mtf_multiply(double* psi, const double* mtf, int64_t plane, int nb,
                                 double inv_s, cudaStream_t s);
 
+// out[p] = sum over r < world of in[r * n + p], added in rank order (FP64):
+// the pixel sums of a sharded raster, the same bits on every rank.
+cudaError_t launch_rank_sum(const double* in, int world, int64_t n, double* out,
+                            cudaStream_t s);
 // acc_a[p] += sum_b |psi_b[p]|, acc_i[p] += sum_b |psi_b[p]|^2 (FP64).
 cudaError_t launch_pixel_accum(bool fp64, const void* psi, int64_t batch_stride,
                                int nb, int64_t npix, double* acc_a, double* acc_i,

@@ -184,9 +184,10 @@ row_split_pipe_kernel(const PassArgs a, int* err) {
 // -------------------------------------------- row pass (split, staged) --
 // The split-wave row pass with its slice tables staged in shared memory.
 // One CTA transforms row i of P probes of the batch (one line each).  On
-// entry thread 0 starts bulk copies of the transmission row tau[i], which
-// the P lines share, and of each probe's vacuum row psi0[(i - sx) mod nx];
-// meanwhile every line loads its scattered row from global memory and runs
+// entry bulk copies of the transmission row tau[i], which the P lines
+// share, and of each probe's vacuum row psi0[(i - sx) mod nx] start (each
+// line issues its own); meanwhile every line loads its scattered row from
+// global memory and runs
 // the inverse transform, so the update then reads tau and psi0 from shared
 // memory with no L2 round trip left on its path.  Arithmetic is that of
 // ROW_SPLIT (split_elem) element for element, so the results are
@@ -231,18 +232,21 @@ row_split_staged_kernel(const PassArgs a, int* err) {
   const int b = b0 + line;
   const int nvalid = a.nb - b0 < P ? a.nb - b0 : P;
   const bool valid = line < nvalid;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0) {  // the barrier expects every byte before any copy starts
     mbar_init(&bar, 1);
     mbar_fence_init();
     mbar_expect_tx(&bar, (uint32_t)((1 + nvalid) * N * 8));
-    bulk_g2s(tau_s, static_cast<const C*>(a.trans) + (int64_t)i * N, N * 8, &bar);
-    for (int l = 0; l < nvalid; ++l) {
-      const int sx = a.shifts[2 * (b0 + l)];
-      const int ix = (i < sx) ? i + a.nx - sx : i - sx;
-      bulk_g2s(psi0_s + l * N, static_cast<const C*>(a.psi0) + (int64_t)ix * N, N * 8, &bar);
-    }
   }
   __syncthreads();
+  // each line's first thread fetches its own probe's shift and vacuum row,
+  // so no thread waits on another's loads
+  if (threadIdx.x == 0)
+    bulk_g2s(tau_s, static_cast<const C*>(a.trans) + (int64_t)i * N, N * 8, &bar);
+  if (t == 0 && valid) {
+    const int sx = a.shifts[2 * b];
+    const int ix = (i < sx) ? i + a.nx - sx : i - sx;
+    bulk_g2s(psi0_s + line * N, static_cast<const C*>(a.psi0) + (int64_t)ix * N, N * 8, &bar);
+  }
   auto sync = [] {
     if constexpr (T <= 32) __syncwarp();
     else __syncthreads();

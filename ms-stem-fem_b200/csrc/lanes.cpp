@@ -28,8 +28,9 @@ constexpr size_t round_up(size_t n, size_t a) { return (n + a - 1) / a * a; }
 
 }  // namespace
 
-Lane::Lane(msf_context* ctx, int nx, int ny, int slots)
-    : ctx_(ctx), nx_(nx), ny_(ny), B_(slots), plane_((int64_t)nx * ny) {}
+Lane::Lane(msf_context* ctx, int nx, int ny, int slots, int priority, bool fair)
+    : ctx_(ctx), nx_(nx), ny_(ny), B_(slots), priority_(priority), fair_(fair),
+      plane_((int64_t)nx * ny) {}
 
 Lane::~Lane() {
   if (stream_) cudaStreamSynchronize(stream_);
@@ -55,7 +56,7 @@ msf_status Lane::init() {
     return MSF_ERR_ARG;
   }
   MSF_CUDA(cudaSetDevice(ctx_->device));
-  MSF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  MSF_CUDA(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, priority_));
   MSF_TRY(ctx_->alloc(&psi_, 8 * (size_t)plane_ * B_));
   // idle slots are still read by the column pass's tile copies
   MSF_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, stream_));
@@ -199,16 +200,21 @@ msf_status Lane::capture_detect() {
 
 msf_status Lane::step() {
   if (!busy()) return MSF_OK;
-  // refill idle slots from the queue, oldest raster first
+  // refill idle slots from the queue: oldest raster first, or (fair) the
+  // raster with the fewest probes in flight
   for (int i = 0; i < B_ && !queue_.empty(); ++i) {
     if (slot_[i].job) continue;
-    SlotJob* j = queue_.front();
+    auto pick = queue_.begin();
+    if (fair_)
+      for (auto it = queue_.begin(); it != queue_.end(); ++it)
+        if ((*it)->started - (*it)->done < (*pick)->started - (*pick)->done) pick = it;
+    SlotJob* j = *pick;
     slot_[i].job = j;
     slot_[i].probe = j->next_probe++;
     slot_[i].s = 0;
     ++j->started;
     ++active_;
-    if (j->next_probe == j->plan.n_probes) queue_.pop_front();
+    if (j->next_probe == j->plan.n_probes) queue_.erase(pick);
   }
 
   // this step's table, in the next free ring entry

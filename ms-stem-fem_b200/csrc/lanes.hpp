@@ -39,7 +39,15 @@ struct SlotJob {
 
 class Lane {
  public:
-  Lane(msf_context* ctx, int nx, int ny, int slots);
+  // `priority`: the CUDA stream priority of the lane's launches (0: the
+  // default; lower numbers are scheduled first).  `fair`: an idle slot takes
+  // the next probe of the raster with the fewest probes in flight (oldest
+  // first among equals), so a raster that arrives while a large one runs
+  // gets its share of the slots at once; otherwise the oldest raster's
+  // probes go first.  Neither changes any result: a probe's arithmetic does
+  // not depend on its slot, and each raster's probes still start, finish
+  // and are detected in probe order.
+  Lane(msf_context* ctx, int nx, int ny, int slots, int priority = 0, bool fair = false);
   ~Lane();
   Lane(const Lane&) = delete;
   Lane& operator=(const Lane&) = delete;
@@ -79,6 +87,8 @@ class Lane {
 
   msf_context* ctx_;
   int nx_, ny_, B_;
+  int priority_ = 0;
+  bool fair_ = false;
   int64_t plane_;
   cudaStream_t stream_ = nullptr;
   DevBuf psi_, table_, partial_, err_;

@@ -2,9 +2,12 @@
 //
 // Submission copies the request into a FIFO and returns a ticket.  A worker
 // thread owns the lanes and loops:
-//   1. admit waiting requests in arrival order while their estimated device
-//      bytes fit the budget (the oldest is always admitted when nothing
-//      runs or builds) and hand them to the builder thread;
+//   1. admit waiting requests in arrival order whose estimated device bytes
+//      fit the budget (the oldest is always admitted when nothing runs or
+//      builds); a request that does not fit lets later, smaller ones past
+//      it until it has waited kBackfillWindow seconds, after which it holds
+//      them back until memory frees up for it; admitted requests go to the
+//      builder thread;
 //   2. hand the probes of every request the builder finished to the lane of
 //      its grid size (created on first use);
 //   3. step every lane that has work and a free table in its ring (no
@@ -14,8 +17,12 @@
 //      on the host), publish their results and latency, free their memory.
 // The builder thread builds specimens and raster plans on a context and
 // stream of its own, so those set-up kernels overlap the lanes' steps
-// instead of holding the worker.  A request that arrives while others run
-// joins the running launches as soon as slots of its grid size free up.
+// instead of holding the worker; it takes the smallest admitted request
+// first (unless one has waited kBackfillWindow seconds).  A request that
+// arrives while others run joins the running launches as soon as slots of
+// its grid size free up: lanes refill slots fairly across their rasters,
+// and lanes of smaller grids run on higher-priority streams, so a small
+// request is not queued behind the launches of a large one.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -36,6 +43,10 @@
 namespace msf {
 namespace {
 
+// Seconds a request that does not fit the budget lets later requests be
+// admitted (or built) before it.
+constexpr double kBackfillWindow = 5.0;
+
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
       .count();
@@ -45,6 +56,7 @@ double now_s() {
 struct Stored {
   msf_status status = MSF_OK;
   std::string error;
+  int32_t nx = 0, ny = 0;  // the request's grid (latency by grid size)
   int64_t n_probes = 0;
   int32_t n_k = 0;
   std::vector<double> adf, k_lower, v[6], mean_a, mean_i, ring_a, ring_i;
@@ -123,6 +135,7 @@ struct msf_server {
   std::set<uint64_t> cancelled;  // admitted requests whose results are discarded
   std::set<uint64_t> live;       // submitted, not yet finished
   std::vector<double> latencies;
+  std::map<std::pair<int, int>, std::vector<double>> latencies_by_grid;
   int64_t submitted = 0, completed = 0, failed = 0, running_n = 0, probe_slices = 0;
   double t_first = -1, t_last = 0;
   int64_t held_bytes = 0;
@@ -142,6 +155,7 @@ struct msf_server {
     if (s.status == MSF_OK) {
       ++completed;
       latencies.push_back(s.latency);
+      latencies_by_grid[{s.nx, s.ny}].push_back(s.latency);
       probe_slices += s.probe_slices;
       t_last = now_s();
     } else {
@@ -184,8 +198,13 @@ struct msf_server {
         std::unique_lock<std::mutex> lk(mu);
         cv_build.wait(lk, [&] { return stopping_builder || !to_build.empty(); });
         if (to_build.empty()) return;
-        p = std::move(to_build.front());
-        to_build.pop_front();
+        // smallest first, unless the oldest has waited the backfill window
+        auto pick = to_build.begin();
+        if (now_s() - pick->r.t_submit < kBackfillWindow)
+          for (auto it = to_build.begin(); it != to_build.end(); ++it)
+            if (it->need < pick->need) pick = it;
+        p = std::move(*pick);
+        to_build.erase(pick);
       }
       p.status = build(p.r, &p.run);
       if (p.status != MSF_OK) p.error = last_error_copy();
@@ -205,9 +224,15 @@ struct msf_server {
     const std::pair<int, int> key{r.grid.nx, r.grid.ny};
     auto it = lanes.find(key);
     if (it == lanes.end()) {
-      const int b = lane_slots(slots, (int64_t)r.grid.nx * r.grid.ny, (int)lanes.size() + 1,
-                               1 << 30);
-      auto lane = std::make_unique<Lane>(ctx, r.grid.nx, r.grid.ny, b);
+      const int64_t plane = (int64_t)r.grid.nx * r.grid.ny;
+      const int b = lane_slots(slots, plane, (int)lanes.size() + 1, 1 << 30);
+      // smaller grids on higher-priority streams: one step per 4x the pixels
+      int least = 0, greatest = 0;
+      cudaDeviceGetStreamPriorityRange(&least, &greatest);
+      int lg = 0;
+      while ((int64_t(1) << (lg + 1)) <= plane) ++lg;
+      const int prio = std::min(least, std::max(greatest, greatest + (lg - 16) / 2));
+      auto lane = std::make_unique<Lane>(ctx, r.grid.nx, r.grid.ny, b, prio, true);
       st = lane->init();
       if (st != MSF_OK) return st;
       it = lanes.emplace(key, std::move(lane)).first;
@@ -219,6 +244,8 @@ struct msf_server {
   void finish(Running& r) {
     Stored s;
     const RasterPlan& P = r.job->plan;
+    s.nx = r.lane->nx();
+    s.ny = r.lane->ny();
     s.n_probes = P.n_probes;
     s.n_k = P.n_k;
     s.adf.assign(P.n_probes, 0.0);
@@ -273,15 +300,20 @@ struct msf_server {
       // 1. admission: to the builder
       {
         std::unique_lock<std::mutex> lk(mu);
-        while (!waiting.empty()) {
-          const int64_t need = estimate_bytes(waiting.front());
+        const double t = now_s();
+        for (auto it = waiting.begin(); it != waiting.end();) {
+          const int64_t need = estimate_bytes(*it);
           const bool idle = running.empty() && to_build.empty() && built.empty();
-          if (!idle && ctx->allocated() + bctx->allocated() + building_bytes + need > budget)
-            break;
+          if (!idle && ctx->allocated() + bctx->allocated() + building_bytes + need > budget) {
+            // does not fit: later requests may pass it while it is young
+            if (t - it->t_submit >= kBackfillWindow) break;
+            ++it;
+            continue;
+          }
           Pending p;
-          p.r = std::move(waiting.front());
+          p.r = std::move(*it);
           p.need = need;
-          waiting.pop_front();
+          it = waiting.erase(it);
           ++running_n;
           building_bytes += need;
           to_build.push_back(std::move(p));
@@ -537,6 +569,32 @@ msf_status msf_server_stats_get(msf_server* s, msf_server_stats* out) {
     st.probe_slices_per_s = (double)s->probe_slices / (s->t_last - s->t_first);
   *out = st;
   return MSF_OK;
+}
+
+int32_t msf_server_grid_stats_get(msf_server* s, msf_server_grid_stats* out, int32_t cap) {
+  if (!s) return 0;
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::vector<std::pair<int64_t, std::pair<int, int>>> grids;
+  for (const auto& kv : s->latencies_by_grid)
+    grids.push_back({(int64_t)kv.first.first * kv.first.second, kv.first});
+  std::sort(grids.begin(), grids.end());
+  for (int32_t k = 0; k < (int32_t)grids.size() && k < cap && out; ++k) {
+    std::vector<double> l = s->latencies_by_grid[grids[k].second];
+    std::sort(l.begin(), l.end());
+    auto q = [&](double f) {
+      const size_t i = (size_t)std::min<double>((double)l.size() - 1, f * (double)l.size());
+      return l[i];
+    };
+    msf_server_grid_stats g{};
+    g.nx = grids[k].second.first;
+    g.ny = grids[k].second.second;
+    g.completed = (int64_t)l.size();
+    g.p50_s = q(0.50);
+    g.p99_s = q(0.99);
+    g.max_s = l.back();
+    out[k] = g;
+  }
+  return (int32_t)grids.size();
 }
 
 msf_status msf_server_cancel(msf_server* s, uint64_t ticket) {

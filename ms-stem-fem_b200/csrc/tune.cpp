@@ -4,7 +4,8 @@
 // batched slice passes: probes per launch, whether the column pass runs as
 // the persistent TMA-pipelined kernel, whether the split-wave row pass
 // stages its slice tables in shared memory, and that row pass's FFT radix
-// schedule (32 elements a thread in two or three stages, or 16 in three).  The winner is kept per context
+// schedule (32 elements a thread in two or three stages, or 16 in three;
+// 8 and 16 at 256 points).  The winner is kept per context
 // and can be saved and reloaded as text, like wisdom.
 #include <cmath>
 #include <cstdio>
@@ -51,16 +52,13 @@ msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
   if (!ctx->pipe_env) {
     const bool col = pipe_supported(g.nx, g.ny, ctx->fp64);
     const bool staged = !ctx->fp64 && staged_row_supported(g.nx, g.ny);
-    pipes = {0};
-    if (col) pipes.push_back(MSF_PIPE_COL);
-    if (staged) {  // both FFT radix schedules of the staged row pass
-      pipes.push_back(MSF_ROW_STAGED);
-      pipes.push_back(MSF_ROW_STAGED | MSF_ROW_ALT);
-    }
-    if (col && staged) {
-      pipes.push_back(MSF_PIPE_COL | MSF_ROW_STAGED);
-      pipes.push_back(MSF_PIPE_COL | MSF_ROW_STAGED | MSF_ROW_ALT);
-    }
+    // column pass plain or pipelined; FP32 row pass plain or staged, each
+    // on either FFT radix schedule
+    std::vector<int> rows{0};
+    if (staged) rows = {0, MSF_ROW_ALT, MSF_ROW_STAGED, MSF_ROW_STAGED | MSF_ROW_ALT};
+    pipes.clear();
+    for (int c : col ? std::vector<int>{0, MSF_PIPE_COL} : std::vector<int>{0})
+      for (int r : rows) pipes.push_back(c | r);
   }
   const int saved_pipe = ctx->pipe;
   ctx->tuned.erase({g.nx, g.ny});  // time_passes then runs ctx->pipe

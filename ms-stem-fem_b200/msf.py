@@ -18,7 +18,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libmsf.so"
 CLI_PATH = HERE / "bin" / "ms-stem-fem"
-ABI_VERSION = 3  # MSF_ABI_VERSION of the include/msf.h these structs mirror
+ABI_VERSION = 4  # MSF_ABI_VERSION of the include/msf.h these structs mirror
 
 MSF_FP64, MSF_FP32 = 0, 1
 OUT_ADF_IMAGE = 1 << 0
@@ -46,8 +46,11 @@ EXPORTED = [
     "msf_server_stats_get", "msf_server_destroy", "msf_segment_count", "msf_run_partial",
     "msf_finish", "msf_run_plain", "msf_amorphous_positions", "msf_run_md", "msf_md_main",
     "msf_tune", "msf_wisdom_export", "msf_wisdom_import", "msf_server_cancel",
-    "msf_specimen_live_columns",
+    "msf_specimen_live_columns", "msf_comm_create", "msf_comm_destroy",
+    "msf_comm_allgather_host", "msf_run_sharded", "msf_server_grid_stats_get",
+    "msf_context_keep_potentials", "msf_specimen_potential",
 ]
+COMM_NCCL, COMM_HOST = 1, 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -106,6 +109,16 @@ class Results(C.Structure):
                 ("correlograph_probes", _dp), ("first_psi", _dp),
                 ("ms_row_pass", C.c_double), ("ms_col_pass", C.c_double),
                 ("pass_batch", C.c_int32)]
+
+
+class GridStats(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("completed", C.c_int64),
+                ("p50_s", C.c_double), ("p99_s", C.c_double), ("max_s", C.c_double)]
+
+
+class ShardInfo(C.Structure):
+    _fields_ = [("p_begin", C.c_int64), ("p_end", C.c_int64), ("seconds_shard", C.c_double),
+                ("seconds_exchange", C.c_double), ("seconds_finish", C.c_double)]
 
 
 class Request(C.Structure):
@@ -205,6 +218,17 @@ def lib() -> C.CDLL:
         L.msf_probe_noalloc.argtypes = [C.POINTER(Grid), C.POINTER(Optics), C.c_void_p,
                                         C.c_void_p]
         L.msf_time_passes.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]
+        L.msf_context_keep_potentials.argtypes = [C.c_void_p, C.c_int32]
+        L.msf_specimen_potential.argtypes = [C.c_void_p, C.c_int32, _dp]
+        L.msf_server_grid_stats_get.argtypes = [C.c_void_p, C.POINTER(GridStats), C.c_int32]
+        L.msf_comm_create.argtypes = [C.c_int32, C.c_int32, C.c_char_p, C.c_int32, C.c_int32,
+                                      C.c_double, C.POINTER(C.c_void_p)]
+        L.msf_comm_destroy.argtypes = [C.c_void_p]
+        L.msf_comm_destroy.restype = None
+        L.msf_comm_allgather_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.msf_run_sharded.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Optics),
+                                      C.POINTER(Raster), C.POINTER(Detect), C.c_void_p,
+                                      C.POINTER(Results), C.POINTER(ShardInfo)]
         if L.msf_abi_version() != ABI_VERSION:
             raise RuntimeError("libmsf.so has ABI version %d, these bindings expect %d: "
                                "rebuild it" % (L.msf_abi_version(), ABI_VERSION))
@@ -311,6 +335,11 @@ class Context:
         _check(lib().msf_context_create(C.byref(opt), C.byref(h)))
         self._h = h
         self.precision = precision
+
+    def keep_potentials(self, on=True):
+        """Specimens built from now on keep their slices' projected
+        potentials (msf_context_keep_potentials; --paptif)."""
+        _check(lib().msf_context_keep_potentials(self._h, 1 if on else 0))
 
     def close(self):
         if getattr(self, "_h", None) is not None:
@@ -439,6 +468,21 @@ class Context:
                 "probe_slices": info.probe_slices, "kernel_launches": info.kernel_launches,
                 "seconds_raster": info.seconds_raster, "n_k": info.n_k}
 
+    def run_sharded(self, spec: "Specimen", optics: Optics, raster: Raster, detect: Detect,
+                    comm: "Comm", want_means=False, cap_k=8192) -> "RunResult":
+        """msf_run over the communicator's ranks (msf_run_sharded): every rank
+        returns the whole raster's ADF image and FEM statistics; `shard` on
+        the result holds this rank's probe range and timings."""
+        nx, ny = spec.grid.nx, spec.grid.ny
+        out = RunResult(raster.n_x * raster.n_y, cap_k, nx, ny, False, want_means)
+        info = ShardInfo()
+        _check(lib().msf_run_sharded(self._h, spec._h, C.byref(optics), C.byref(raster),
+                                     C.byref(detect), comm._h, C.byref(out._struct),
+                                     C.byref(info)))
+        out.finish(raster, detect)
+        out.shard = {f: getattr(info, f) for f, _ in ShardInfo._fields_}
+        return out
+
     def time_passes(self, spec: "Specimen", nb: int, reps: int = 10):
         """Mean ms per launch of the fused row and column slice passes."""
         r, c = C.c_double(), C.c_double()
@@ -484,6 +528,61 @@ def finish(grid: Grid, optics: Optics, raster: Raster, detect: Detect, amp, inte
     return out
 
 
+def _prefer_framework_nccl():
+    """Point the library at the NCCL of the Python environment's `nvidia-nccl`
+    wheel (the one torch links against) unless MSF_NCCL_LIBRARY is set, so
+    that a later `import torch` in this process finds the NCCL it expects."""
+    if os.environ.get("MSF_NCCL_LIBRARY"):
+        return
+    import importlib.util
+    try:
+        spec = importlib.util.find_spec("nvidia.nccl")
+    except (ImportError, ValueError):
+        spec = None
+    for base in (spec.submodule_search_locations if spec else None) or []:
+        path = os.path.join(base, "lib", "libnccl.so.2")
+        if os.path.exists(path):
+            os.environ["MSF_NCCL_LIBRARY"] = path
+            return
+
+
+class Comm:
+    """A communicator of `world` ranks (msf_comm_create): rank 0 listens at
+    `rendezvous` ("host:port"), the others connect; transport COMM_NCCL
+    (device buffers, one GPU per rank) or COMM_HOST (through the bootstrap
+    connections).  Collective: every rank creates one."""
+
+    def __init__(self, rank: int, world: int, rendezvous: str = "", transport: int = COMM_HOST,
+                 device: int = -1, timeout_s: float = 60.0):
+        if transport == COMM_NCCL:
+            _prefer_framework_nccl()
+        h = C.c_void_p()
+        _check(lib().msf_comm_create(rank, world, rendezvous.encode(), transport, device,
+                                     timeout_s, C.byref(h)))
+        self._h = h
+        self.rank, self.world = rank, world
+
+    def allgather(self, a: np.ndarray) -> np.ndarray:
+        """Every rank's `a` (same shape and dtype on all ranks), stacked in
+        rank order."""
+        a = np.ascontiguousarray(a)
+        out = np.empty((self.world,) + a.shape, dtype=a.dtype)
+        _check(lib().msf_comm_allgather_host(self._h, a.ctypes.data, a.nbytes,
+                                             out.ctypes.data))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().msf_comm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """Request loop with continuous batching (msf_server_*), FP32 wavefields."""
 
@@ -526,6 +625,14 @@ class Server:
         s = ServerStats()
         _check(lib().msf_server_stats_get(self._h, C.byref(s)))
         return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def grid_stats(self) -> list:
+        """Latency per grid size of the completed requests
+        (msf_server_grid_stats_get), in order of grid size."""
+        n = lib().msf_server_grid_stats_get(self._h, None, 0)
+        arr = (GridStats * max(n, 1))()
+        n = lib().msf_server_grid_stats_get(self._h, arr, n)
+        return [{f: getattr(arr[k], f) for f, _ in GridStats._fields_} for k in range(n)]
 
     def close(self):
         if getattr(self, "_h", None) is not None:
@@ -570,6 +677,13 @@ class Specimen:
     def transmission(self, s: int) -> np.ndarray:
         out = np.zeros(2 * self.grid.nx * self.grid.ny)
         _check(lib().msf_specimen_transmission(self._h, s, _p(out)))
+        return out.reshape(self.grid.nx, self.grid.ny, 2)
+
+    def potential(self, s: int) -> np.ndarray:
+        """Slice s's projected potential before the exponential
+        (msf_specimen_potential; the context must keep potentials)."""
+        out = np.zeros(2 * self.grid.nx * self.grid.ny)
+        _check(lib().msf_specimen_potential(self._h, s, _p(out)))
         return out.reshape(self.grid.nx, self.grid.ny, 2)
 
     def device_bytes(self) -> int:

@@ -1,0 +1,61 @@
+"""Serving-loop scheduling (msf_server): a small request that arrives just
+after a large one is not queued behind it, whether it needs a lane of its
+own (a smaller grid: higher-priority stream) or shares the large one's lane
+(same grid: slots shared fairly across rasters); latency is reported per
+grid size; and the shared slots change no result (bit-identical to the
+request run alone)."""
+import time
+
+import numpy as np
+import pytest
+
+import msf
+from test_gpu_slots import JobSpec
+
+pytestmark = pytest.mark.gpu
+
+
+def _wait(srv, tickets):
+    out = {}
+    while len(out) < len(tickets):
+        for t in tickets:
+            if t not in out:
+                r = srv.poll(t, wait_ms=5)
+                if r is not None:
+                    out[t] = (r, time.time())
+    return out
+
+
+def _submit(srv, j):
+    return srv.submit(j.grid, j.pos, j.z, j.optics, j.raster, j.detect)
+
+
+@pytest.mark.parametrize("small_n", [256, 512])
+def test_small_request_finishes_before_the_large_one_ahead_of_it(small_n):
+    big = JobSpec(512, 50.0, 60.0, 6000, seed=61, raster_n=40)    # 1600 probes, ~30 slices
+    box = 25.0 if small_n == 256 else 50.0
+    small = JobSpec(small_n, box, 6.0, 150 if small_n == 256 else 600, seed=62, raster_n=2)
+    srv = msf.Server(slots=64)
+    warm = _submit(srv, JobSpec(small_n, box, 4.0, 50, seed=63, raster_n=1))
+    _wait(srv, [warm])
+    t0 = time.time()
+    tb = _submit(srv, big)
+    ts = _submit(srv, small)
+    done = _wait(srv, [tb, ts])
+    t_big, t_small = done[tb][1] - t0, done[ts][1] - t0
+    print("grid %d after 512^2 x 1600 probes: small %.3f s, large %.3f s"
+          % (small_n, t_small, t_big))
+    assert t_small < 0.5 * t_big
+    alone = msf.Server(slots=64)
+    ta = _submit(alone, small)
+    ref = _wait(alone, [ta])[ta][0]
+    got = done[ts][0]
+    assert np.array_equal(got.adf_image, ref.adf_image)
+    for m, v in ref.v.items():
+        assert np.array_equal(got.v[m], v, equal_nan=True), m
+    grids = {(g["nx"], g["ny"]): g for g in srv.grid_stats()}
+    assert (512, 512) in grids and (small_n, small_n) in grids
+    g = grids[(small_n, small_n)]
+    assert g["completed"] == 2 and 0 < g["p50_s"] <= g["p99_s"] <= g["max_s"]
+    srv.close()
+    alone.close()

@@ -42,10 +42,12 @@ def test_staged_row_pass_is_bit_identical(name, batch, col, golden_tmp):
         assert np.array_equal(staged.v[m], v, equal_nan=True), m
 
 
+@pytest.mark.parametrize("pipe", [1 | 8, 1 | 4 | 8])
 @pytest.mark.parametrize("name,batch", [("g512", 5), ("c2_small", 3), ("g2048", 7)])
-def test_alternative_schedule_matches_reference(name, batch, golden_tmp):
+def test_alternative_schedule_matches_reference(name, batch, pipe, golden_tmp):
+    """The 16-element radix schedule, in the plain and the staged row pass."""
     meta, ref = load_case(name)
-    res = _run(name, golden_tmp, 1 | 4 | 8, batch)
+    res = _run(name, golden_tmp, pipe, batch)
     if "adf_image" in ref:
         assert rel_err(res.adf_image, ref["adf_image"]).max() <= 1e-4
     for m in ("V_omega", "V_re"):
