@@ -77,21 +77,29 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(which, name="row_col_pass_1024_fp32.md"):
-    """DRAM bytes per launch of the row or column pass ("row" / "col") from
-    the committed ncu summary (profiles/), or None before one was captured."""
-    p = ROOT / "profiles" / name
-    if not p.exists():
-        return None
-    key = "traffic_bytes_per_launch_%s:" % which
-    for line in p.read_text().splitlines():
-        if line.startswith(key):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
-
+def ncu_traffic(which, nb):
+    """DRAM bytes per launch of the row or column pass ("row" / "col") at nb
+    probes per launch, from the committed ncu summaries (profiles/*.md): a
+    figure captured at nb itself when one exists, else the 32-probe capture
+    scaled by nb / 32 (DRAM bytes grow in proportion to the probes a launch
+    carries).  Returns (bytes, how) or (None, None)."""
+    exact = "traffic_bytes_per_launch_%s_b%d:" % (which, nb)
+    base = "traffic_bytes_per_launch_%s:" % which
+    found = {}
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        for line in p.read_text().splitlines():
+            for key in (exact, base):
+                if line.startswith(key) and key not in found:
+                    try:
+                        found[key] = (float(line.split(":", 1)[1].split()[0]), p.name)
+                    except ValueError:
+                        pass
+    if exact in found:
+        return found[exact][0], "ncu capture at %d probes per launch (%s)" % (nb, found[exact][1])
+    if base in found:
+        return (found[base][0] * nb / 32.0,
+                "ncu capture at 32 probes per launch scaled by %d/32 (%s)" % (nb, found[base][1]))
+    return None, None
 
 def plain_and_precision(msf, job, q, z, device, argv_sample, res32):
     """The two comparisons the headline metric is quoted with.
@@ -667,9 +675,8 @@ def main():
     t_dom = max(ms_row, ms_col) * 1e-3
     peak, peak_kind = measured_peaks()
     achieved = alg / t_dom / 1e9
-    traffic = ncu_traffic(dom) if (n == 1024 and args.precision == "fp32") else None
-    if traffic is not None:
-        traffic *= nb / 32.0
+    traffic, traffic_src = (ncu_traffic(dom, nb) if (n == 1024 and args.precision == "fp32")
+                            else (None, None))
     # the flop ceiling beside the HBM one: two complex 2-D FFTs at
     # 5 n log2 n plus the point-wise work, per probe*slice, against the
     # FP32 CUDA-core peak (SMs x 128 lanes x 2 flops x max SM clock;
@@ -688,6 +695,7 @@ def main():
                           (dom, "transmission" if dom == "row" else "propagator", nb),
                 "peak_source": peak_kind, "ms_row": round(ms_row, 4), "ms_col": round(ms_col, 4),
                 "algorithmic_bytes_per_launch": alg, "live_column_fraction": round(live, 4),
+                "traffic_source": traffic_src,
                 "timing": timing}
 
     # end to end through the C ABI from host buffers

@@ -56,6 +56,8 @@ def test_small_request_finishes_before_the_large_one_ahead_of_it(small_n):
     grids = {(g["nx"], g["ny"]): g for g in srv.grid_stats()}
     assert (512, 512) in grids and (small_n, small_n) in grids
     g = grids[(small_n, small_n)]
-    assert g["completed"] == 2 and 0 < g["p50_s"] <= g["p99_s"] <= g["max_s"]
+    # the warm-up request and the small one (and, at 512^2, the large one)
+    assert g["completed"] == (3 if small_n == 512 else 2)
+    assert 0 < g["p50_s"] <= g["p99_s"] <= g["max_s"]
     srv.close()
     alone.close()
