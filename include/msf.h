@@ -250,7 +250,8 @@ typedef struct {
                                  pass, bit 1 pipelined row pass, bit 2 row
                                  pass with staged slice tables (FP32), bit 3
                                  the FP32 split-wave row pass on its
-                                 alternative FFT radix schedule             */
+                                 alternative FFT radix schedule, bit 4 the
+                                 plain row pass prefetching its tables      */
   double ns_per_probe_slice;  /* measured time of the two slice passes        */
 } msf_tuning;
 /* Times the two slice passes of `spec`'s grid (CUDA events, after a

@@ -551,6 +551,7 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
     col.live_groups = spec->live_groups.as<int32_t>();
     col.n_live_groups = spec->n_live_groups;
   }
+  row.prefetch_tables = (pipe & MSF_ROW_PREFETCH) ? 1 : 0;
   PassArgs row_staged = row;  // schedule 1 reads the zero bits in its own layout
   if (row_sched == 1 && row.row_dead_bits) row_staged.row_dead_bits = spec->dead_bits_alt.as<uint32_t>();
   auto row_pass = [&]() {
@@ -1088,6 +1089,7 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   MSF_TRY(ctx->twiddles(g.ny, fp64, &row.tw));
   MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
   row.inv_s = col.inv_s = 1.0 / g.s;
+  row.prefetch_tables = (!fp64 && (pipe & MSF_ROW_PREFETCH)) ? 1 : 0;
   row.probe = P.probe64.p;
   row.first_scale = g.nxny / g.s;
   col.mask_lo = spec->mask_lo.as<int32_t>();

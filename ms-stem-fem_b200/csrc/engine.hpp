@@ -73,7 +73,11 @@ constexpr int MSF_PIPE_COL = 1, MSF_PIPE_ROW = 2, MSF_ROW_STAGED = 4;
 // the split-wave row pass's alternative FFT radix schedule (16 elements a
 // thread; staged or plain)
 constexpr int MSF_ROW_ALT = 8;
-constexpr int MSF_PIPE_ALL = MSF_PIPE_COL | MSF_PIPE_ROW | MSF_ROW_STAGED | MSF_ROW_ALT;
+// the plain split-wave row pass prefetches its transmission and vacuum rows
+// into L1 (PassArgs::prefetch_tables)
+constexpr int MSF_ROW_PREFETCH = 16;
+constexpr int MSF_PIPE_ALL =
+    MSF_PIPE_COL | MSF_PIPE_ROW | MSF_ROW_STAGED | MSF_ROW_ALT | MSF_ROW_PREFETCH;
 
 struct msf_context {
   int device = 0;

@@ -99,6 +99,22 @@ constexpr int col_cols() {
 }
 
 // ------------------------------------------------------------ row pass ---
+// A load that does not allocate in L1 (the wavefield is read once a pass),
+// and a prefetch of one 128-byte line into L1.
+template <typename C>
+__device__ __forceinline__ C ld_stream(const C* p) {
+  if constexpr (sizeof(C) == 8) {
+    float2 v;
+    asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+  } else {
+    return *p;
+  }
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Split-wave transmission step (split_elem) on one row held in registers
 // (element t + T*m of row i); psi0 is the probe's vacuum wave, shifted like
 // the probe.
@@ -210,9 +226,26 @@ row_kernel(const PassArgs a) {
     // columns removed by the band limit were not stored: they are zero
     const uint32_t skip = (a.row_dead_bits && (a.row_dead_io & 1)) ? __ldg(a.row_dead_bits + t)
                                                                   : 0u;
+    if (OP == ROW_SPLIT && a.prefetch_tables) {
 #pragma unroll
-    for (int m = 0; m < E; ++m)
-      v[m] = ((skip >> m) & 1u) ? C{(Real)0, (Real)0} : row[t + T * m];
+      for (int m = 0; m < E; ++m)
+        v[m] = ((skip >> m) & 1u) ? C{(Real)0, (Real)0} : ld_stream(row + t + T * m);
+      // the line's tau row and (shifted) vacuum row: 128-byte lines spread
+      // over the line's threads, issued after the wavefield loads
+      constexpr int kLines = N * (int)sizeof(C) / 128;
+      const int sx = a.shifts[2 * b];
+      const int ix = (i < sx) ? i + a.nx - sx : i - sx;
+      const char* trow = static_cast<const char*>(a.trans) + (int64_t)i * N * sizeof(C);
+      const char* prow = static_cast<const char*>(a.psi0) + (int64_t)ix * N * sizeof(C);
+      for (int l = t; l < kLines; l += T) {
+        prefetch_l1(trow + 128 * l);
+        prefetch_l1(prow + 128 * l);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; ++m)
+        v[m] = ((skip >> m) & 1u) ? C{(Real)0, (Real)0} : row[t + T * m];
+    }
   } else {
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = row[t + T * m];

@@ -3,7 +3,8 @@
 // at 1748-1765).  Here what is measured per grid is the tiling of the
 // batched slice passes: probes per launch, whether the column pass runs as
 // the persistent TMA-pipelined kernel, whether the split-wave row pass
-// stages its slice tables in shared memory, and that row pass's FFT radix
+// stages its slice tables in shared memory (or prefetches them into L1), and
+// that row pass's FFT radix
 // schedule (32 elements a thread in two or three stages, or 16 in three;
 // 8 and 16 at 256 points).  The winner is kept per context
 // and can be saved and reloaded as text, like wisdom.
@@ -55,7 +56,8 @@ msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
     // column pass plain or pipelined; FP32 row pass plain or staged, each
     // on either FFT radix schedule
     std::vector<int> rows{0};
-    if (staged) rows = {0, MSF_ROW_ALT, MSF_ROW_STAGED, MSF_ROW_STAGED | MSF_ROW_ALT};
+    if (staged)
+      rows = {0, MSF_ROW_PREFETCH, MSF_ROW_ALT, MSF_ROW_STAGED, MSF_ROW_STAGED | MSF_ROW_ALT};
     pipes.clear();
     for (int c : col ? std::vector<int>{0, MSF_PIPE_COL} : std::vector<int>{0})
       for (int r : rows) pipes.push_back(c | r);

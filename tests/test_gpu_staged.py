@@ -32,10 +32,13 @@ def _run(name, golden_tmp, pipe, batch):
 
 
 @pytest.mark.parametrize("name,batch", [("g512", 5), ("c2_small", 3), ("g2048", 7)])
+@pytest.mark.parametrize("variant", [4, 16])
 @pytest.mark.parametrize("col", [0, 1])
-def test_staged_row_pass_is_bit_identical(name, batch, col, golden_tmp):
+def test_staged_row_pass_is_bit_identical(name, batch, col, variant, golden_tmp):
+    """variant 4: the staged row pass; 16: the plain one prefetching its
+    tables into L1."""
     plain = _run(name, golden_tmp, col, batch)
-    staged = _run(name, golden_tmp, col | 4, batch)
+    staged = _run(name, golden_tmp, col | variant, batch)
     if plain.adf_image is not None:
         assert np.array_equal(staged.adf_image, plain.adf_image)
     for m, v in plain.v.items():
