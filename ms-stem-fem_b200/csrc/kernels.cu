@@ -164,23 +164,12 @@ row_kernel(const PassArgs a) {
     // slot batch: this CTA's probe reads its own slice tables.  The row
     // loads wait for the slot entry, so a CTA takes nx / (LINES * gridDim.y)
     // consecutive row groups of its slot and pays that wait once.
+    const SlotPass sp = a.slots[b];
+    if (sp.op == SLOT_IDLE) return;
     // columns the band limit removes entirely (when the lane skips them):
     // never loaded, stored (as zeros) only at the slot's last slice
     const uint32_t dead = a.row_dead_bits ? __ldg(a.row_dead_bits + t) : 0u;
     const int groups = a.nx / (LINES * (int)gridDim.y);
-    // the first row group's loads go out together with the slot entry's
-    // (the row's address does not depend on it); an idle slot's or a first
-    // slice's loaded values are then discarded
-    {
-      const int ir = (int)blockIdx.y * groups * LINES + line;
-      const C* rrow = static_cast<const C*>(a.psi) + (int64_t)b * a.batch_stride +
-                      (int64_t)ir * N;
-#pragma unroll
-      for (int m = 0; m < E; ++m)
-        v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : rrow[t + T * m];
-    }
-    const SlotPass sp = a.slots[b];
-    if (sp.op == SLOT_IDLE) return;
     for (int r = 0; r < groups; ++r) {
       const int ir = ((int)blockIdx.y * groups + r) * LINES + line;
       C* rrow = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)ir * N;
@@ -188,11 +177,9 @@ row_kernel(const PassArgs a) {
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = C{(Real)0, (Real)0};
       } else {
-        if (r > 0) {
 #pragma unroll
-          for (int m = 0; m < E; ++m)
-            v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : rrow[t + T * m];
-        }
+        for (int m = 0; m < E; ++m)
+          v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : rrow[t + T * m];
         fft_line<Sh, true>(v, sm, t, tw, sync);
       }
       split_update<Sh>(v, static_cast<const C*>(sp.psi0), static_cast<const C*>(sp.trans),
