@@ -164,7 +164,14 @@ row_kernel(const PassArgs a) {
     // slot batch: this CTA's probe reads its own slice tables.  The row
     // loads wait for the slot entry, so a CTA takes nx / (LINES * gridDim.y)
     // consecutive row groups of its slot and pays that wait once.
-    const SlotPass sp = a.slots[b];
+    // The entry is staged in shared memory and its fields re-read where
+    // they are used (volatile), instead of living in registers across the
+    // transforms, where they pushed the 512- and 1024-point passes into
+    // spills (the plain passes read the same values from kernel parameters).
+    __shared__ SlotPass sp_smem;
+    if (threadIdx.x == 0) sp_smem = a.slots[b];
+    __syncthreads();
+    const volatile SlotPass& sp = sp_smem;
     if (sp.op == SLOT_IDLE) return;
     // columns the band limit removes entirely (when the lane skips them):
     // never loaded, stored (as zeros) only at the slot's last slice
@@ -179,17 +186,33 @@ row_kernel(const PassArgs a) {
       } else {
 #pragma unroll
         for (int m = 0; m < E; ++m)
-          v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0} : rrow[t + T * m];
-        fft_line<Sh, true>(v, sm, t, tw, sync);
+          v[m] = ((dead >> m) & 1u) ? C{(Real)0, (Real)0}
+                 : a.prefetch_tables ? ld_stream(rrow + t + T * m)
+                                     : rrow[t + T * m];
       }
+      if (a.prefetch_tables) {  // this row's tables into L1 during the inverse FFT
+        constexpr int kLines = N * (int)sizeof(C) / 128;
+        const int ix = (ir < sp.sx) ? ir + a.nx - sp.sx : ir - sp.sx;
+        const char* trow = static_cast<const char*>(sp.trans) + (int64_t)ir * N * sizeof(C);
+        const char* prow = static_cast<const char*>(sp.psi0) + (int64_t)ix * N * sizeof(C);
+        for (int l = t; l < kLines; l += T) {
+          prefetch_l1(trow + 128 * l);
+          prefetch_l1(prow + 128 * l);
+        }
+      }
+      if (sp.op != SLOT_FIRST) fft_line<Sh, true>(v, sm, t, tw, sync);
       split_update<Sh>(v, static_cast<const C*>(sp.psi0), static_cast<const C*>(sp.trans),
                        a.nx, ir, t, sp.sx, sp.sy, (Real)a.inv_s);
       fft_line<Sh, false>(v, sm, t, tw, sync);
+      const bool last = sp.last != 0;
+      // the removed-column bits again (an L1 hit) rather than a register
+      // held across both transforms
+      const uint32_t dead_st = a.row_dead_bits ? __ldg(a.row_dead_bits + t) : 0u;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
-        if (!((dead >> m) & 1u))
+        if (!((dead_st >> m) & 1u))
           rrow[t + T * m] = v[m];
-        else if (sp.last)
+        else if (last)
           rrow[t + T * m] = C{(Real)0, (Real)0};
       }
     }

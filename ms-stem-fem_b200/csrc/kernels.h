@@ -120,9 +120,10 @@ struct PassArgs {
   // such columns: it walks live_groups[n_live_groups] (nullptr: all groups)
   const int32_t* live_groups = nullptr;
   int n_live_groups = 0;
-  // split-wave row pass (ROW_SPLIT): prefetch the line's transmission and
-  // vacuum rows into L1 at the start, and load the wavefield past L1, so the
-  // update after the inverse transform finds its tables in L1
+  // split-wave row passes (ROW_SPLIT, ROW_SLOTS): prefetch the line's
+  // transmission and vacuum rows into L1 at the start, and load the
+  // wavefield past L1, so the update after the inverse transform finds its
+  // tables in L1
   int prefetch_tables = 0;
 };
 

@@ -79,6 +79,7 @@ msf_status Lane::init() {
   MSF_TRY(ctx_->twiddles(ny_, false, &row_.tw));
   MSF_TRY(ctx_->twiddles(nx_, false, &col_.tw));
   row_.slots = col_.slots = static_cast<const SlotPass*>(table_.p);
+  row_.prefetch_tables = (ctx_->pipe & MSF_ROW_PREFETCH) ? 1 : 0;
   slot_.assign(B_, Slot{});
   return MSF_OK;
 }

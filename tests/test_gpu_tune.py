@@ -74,3 +74,25 @@ def test_run_reports_pass_times_of_its_first_batch():
     assert r.pass_batch == 16
     assert r.ms_row_pass > 0 and r.ms_col_pass > 0
     assert r.ms_row_pass + r.ms_col_pass < 1e3 * r.seconds_raster
+
+
+def test_kernel_attributes_are_set_on_every_device():
+    """Large-shared-memory launches (FP64 2048-point passes) on a second
+    device after the first: the dynamic shared-memory limit is raised per
+    device, so both runs succeed and agree.  Needs two visible GPUs."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    lam, _ = msf.wavelength(300000.0)
+    g = msf.Grid(nx=2048, ny=2048, voltage=300000.0, xperiod=200.0, yperiod=200.0,
+                 zperiod=10.0, dupe_x=1, dupe_y=1, dupe_z=1, replicate_atoms=0, min_slice=2.0)
+    o = msf.Optics(corrected=0, cs3=1.3e7, cs5=0.0, defocus=0.87 * np.sqrt(1.3e7 * lam),
+                   alpha_max=0.0084)
+    probes = []
+    for dev in (0, 1, 0):
+        ctx = msf.Context(device=dev, precision="fp64")
+        spec = ctx.specimen(g, np.zeros((0, 3)), np.zeros(0, dtype=np.uint32))
+        probes.append(ctx.probe(spec, o))
+        spec.close()
+        ctx.close()
+    assert np.array_equal(probes[0], probes[1]) and np.array_equal(probes[0], probes[2])
