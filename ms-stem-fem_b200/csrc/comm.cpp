@@ -378,13 +378,15 @@ msf_status run_sharded(msf_context* ctx, const msf_specimen* spec, const msf_opt
   const int64_t plane = (int64_t)g.nx * g.ny;
   const bool pix = det->outputs & (MSF_OUT_V_RE | MSF_OUT_OMEGA_VIMAGE | MSF_OUT_V_GT17 |
                                    MSF_OUT_V_RBAR);
-  Rings rings;
+  static const Rings no_rings;
+  std::shared_ptr<const Rings> rings_sp;
   int n_seg = 1;  // ring bins (and correlograph cells), then the ADF annulus
   if (det->outputs & MSF_OUT_FEM_MASK) {
-    rings = make_rings(g, det->dr);
-    n_seg = rings.n_k + 1;
-    if (det->outputs & MSF_OUT_CORRELOGRAPH) n_seg += rings.n_k * make_cells(g, rings).n_phi;
+    rings_sp = rings_for(ctx, g, det->dr);
+    n_seg = rings_sp->n_k + 1;
+    if (det->outputs & MSF_OUT_CORRELOGRAPH) n_seg += rings_sp->n_k * make_cells(g, *rings_sp).n_phi;
   }
+  const Rings& rings = rings_sp ? *rings_sp : no_rings;
   const size_t row_doubles = (size_t)rows_max * n_seg;  // one of amp / inten, padded
 
   // this rank's probes

@@ -283,6 +283,7 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
                               pref, g.bw_pap * g.bw_pap, g.xmin, g.ymin, ctx->stream));
   }
   // slicing (slice.cpp:469-980) and per-atom pixel snaps (slice.cpp:1556-1572)
+  auto host_prep = std::make_unique<TraceScope>("specimen_host_prep");
   Slicing sl = slice_atoms(n, q.data(), g.zmin, g.zpd, gin->min_slice);
   // which slices take the FFT convolution for their potential
   std::vector<uint8_t> by_fft(sl.n(), 0);
@@ -393,7 +394,9 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
     }
   }
 
+  host_prep.reset();
   // transmission functions (slice.cpp:1544-1757)
+  auto trans_scope = std::make_unique<TraceScope>("specimen_transmission");
   const size_t cbytes = ctx->fp64 ? 16 : 8;
   MSF_TRY(ctx->alloc(&spec->t, cbytes * plane * std::max<int64_t>(1, sl.n())));
   DevBuf scratch;
@@ -450,6 +453,8 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
                                        ctx->stream));
   }
 
+  if (trace_enabled()) MSF_CUDA(cudaStreamSynchronize(ctx->stream));  // device time in the record
+  trans_scope.reset();
   // propagators (slice.cpp:1293-1363)
   spec->hprop.clear();
   for (int64_t s = 0; s < sl.n(); ++s) {
@@ -609,6 +614,17 @@ int64_t raster_plan_bytes(const msf_specimen* spec, bool fp64, int64_t n_probes,
   return b;
 }
 
+std::shared_ptr<const Rings> rings_for(msf_context* ctx, const Grid& g, double dr) {
+  const msf_context::RingKey key{g.nx, g.ny, g.xpd, g.ypd, g.bw_t, dr};
+  std::lock_guard<std::mutex> lock(ctx->ring_mu);
+  auto it = ctx->ring_cache.find(key);
+  if (it != ctx->ring_cache.end()) return it->second;
+  auto r = std::make_shared<const Rings>(make_rings(g, dr));
+  if (ctx->ring_cache.size() >= 16) ctx->ring_cache.clear();  // bound the host memory
+  ctx->ring_cache.emplace(key, r);
+  return r;
+}
+
 msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_optics* optics,
                        const msf_raster* raster, const msf_detect* det, RasterPlan* P,
                        int64_t p_begin, int64_t p_end) {
@@ -707,12 +723,12 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
   MSF_TRY(upload(ctx, &P->d_shifts, P->shifts));
 
   // segments: ring bins (FEM) then the ADF detector annulus
-  if (P->fem) P->rings = make_rings(g, det->dr);
-  P->n_k = P->fem ? P->rings.n_k : 0;
+  if (P->fem) P->rings = rings_for(ctx, g, det->dr);
+  P->n_k = P->fem ? P->rings->n_k : 0;
   std::vector<int32_t> seg_idx, seg_start{0};
   if (P->fem) {
-    seg_idx = P->rings.pix;
-    for (int k = 0; k < P->n_k; ++k) seg_start.push_back(P->rings.start[k + 1]);
+    seg_idx = P->rings->pix;
+    for (int k = 0; k < P->n_k; ++k) seg_start.push_back(P->rings->start[k + 1]);
   }
   const std::vector<int32_t> adf_pix =
       detector_pixels(g, det->det_inner / g.lambda, det->det_outer / g.lambda);
@@ -721,7 +737,7 @@ msf_status plan_raster(msf_context* ctx, const msf_specimen* spec, const msf_opt
   P->n_seg = P->n_k + 1;
   if (P->fem && (det->outputs & MSF_OUT_CORRELOGRAPH)) {
     // correlograph cells (k bin, phi bin) after the ADF annulus
-    const Cells cells = make_cells(g, P->rings);
+    const Cells cells = make_cells(g, *P->rings);
     const size_t n_cells = (size_t)P->n_k * cells.n_phi;
     const int32_t base = (int32_t)seg_idx.size();
     seg_idx.insert(seg_idx.end(), cells.pix.begin(), cells.pix.end());
@@ -877,7 +893,9 @@ msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t str
   MSF_TRY(download_sums(ctx, P, stream, amp.data(), inten.data(),
                         P.pix_modes ? acc_a.data() : nullptr,
                         P.pix_modes ? acc_i.data() : nullptr));
-  return finish_host(P.spec->g, P.rings, P.optics, P.det, P.n_probes, amp.data(),
+  static const Rings no_rings;
+  return finish_host(P.spec->g, P.rings ? *P.rings : no_rings, P.optics, P.det, P.n_probes,
+                     amp.data(),
                      inten.data(), P.pix_modes ? acc_a.data() : nullptr,
                      P.pix_modes ? acc_i.data() : nullptr, res);
 }
