@@ -63,12 +63,15 @@ Slicing slice_atoms(int64_t n, const double* q, double zmin, double zperiod,
     sl.thickness = {zperiod};
     return sl;
   }
-  sl.order.resize(n);
-  std::iota(sl.order.begin(), sl.order.end(), 0);
   // scatterer_sorting_lt_z (scatterer.hpp:192); ties share a slice and a
-  // mean, so their order is immaterial -- keep index order.
-  std::stable_sort(sl.order.begin(), sl.order.end(),
-                   [&](int64_t a, int64_t b) { return q[3 * a + 2] < q[3 * b + 2]; });
+  // mean, so their order is immaterial -- keep index order.  Sorting
+  // contiguous (z, index) pairs lexicographically gives exactly that order
+  // (a stable sort by z) without chasing q through an indirect comparator.
+  std::vector<std::pair<double, int64_t>> keys((size_t)n);
+  for (int64_t k = 0; k < n; ++k) keys[(size_t)k] = {q[3 * k + 2], k};
+  std::sort(keys.begin(), keys.end());
+  sl.order.resize(n);
+  for (int64_t k = 0; k < n; ++k) sl.order[(size_t)k] = keys[(size_t)k].second;
   sl.start.push_back(0);
   sl.lower.push_back(0.0);
   double first = q[3 * sl.order[0] + 2];
