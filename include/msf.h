@@ -251,14 +251,22 @@ typedef struct {
                                  pass with staged slice tables (FP32), bit 3
                                  the FP32 split-wave row pass on its
                                  alternative FFT radix schedule, bit 4 the
-                                 plain row pass prefetching its tables      */
+                                 plain row pass prefetching its tables into
+                                 L1, bit 5 the plain row pass prefetching
+                                 the wavefield rows of the CTAs one resident
+                                 wave ahead into L2 (distance scaled by the
+                                 MSF_ROW_AHEAD_PCT environment variable,
+                                 percent of a wave, default 100), bit 6 the
+                                 plain row pass giving each CTA one row of
+                                 consecutive probes                         */
   double ns_per_probe_slice;  /* measured time of the two slice passes        */
 } msf_tuning;
 /* Times the two slice passes of `spec`'s grid (CUDA events, after a
  * warm-up) for each candidate probes-per-launch (8 .. 256, within half the
  * free memory) and each slice-pass variant the grid supports (pipelined
  * column pass or not; for FP32, staged row pass or not, in either FFT radix
- * schedule); records the fastest per probe*slice
+ * schedule, and the plain one with or without its L1 and L2 prefetches);
+ * records the fastest per probe*slice
  * in the context, where msf_run / msf_run_md / msf_run_partial use it for
  * that grid unless the context's batch or MSF_PIPE fixes the choice. */
 msf_status msf_tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out);

@@ -1,4 +1,5 @@
 // extern "C" entry points of libmsf.so (declared in include/msf.h).
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -81,6 +82,7 @@ msf_status msf_context_create(const msf_options* opt, msf_context** out) {
     c->pipe = std::atoi(p);
     c->pipe_env = true;
   }
+  if (const char* p = std::getenv("MSF_ROW_AHEAD_PCT")) c->row_ahead_pct = std::max(1, std::atoi(p));
   if (const char* p = std::getenv("MSF_POTENTIAL"))
     c->potential = std::string(p) == "direct" ? 1 : std::string(p) == "fft" ? 2 : 0;
   c->budget = o.hbm_budget;

@@ -392,6 +392,18 @@ msf_status build_specimen(msf_context* ctx, const msf_grid* gin, const msf_atoms
       spec->h_dead_bits = bits;
       spec->h_live_groups = groups;
     }
+    // live element ranges of a row: [0, d0) and [d1, ny) around one run of
+    // removed columns [d0, d1), widened to even bounds
+    const int d0 = (int)(std::find(dead.begin(), dead.end(), 1) - dead.begin());
+    int d1 = d0;
+    while (d1 < g.ny && dead[d1]) ++d1;
+    const bool one_run = d0 < g.ny && std::find(dead.begin() + d1, dead.end(), 1) == dead.end();
+    const int a1 = one_run ? std::min(g.ny, (d0 + 1) & ~1) : g.ny;
+    const int b0 = one_run ? (d1 & ~1) : g.ny;
+    spec->row_live[0] = 0;
+    spec->row_live[1] = a1;
+    spec->row_live[2] = std::max(a1, b0);
+    spec->row_live[3] = one_run ? g.ny : spec->row_live[2];
   }
 
   host_prep.reset();
@@ -503,6 +515,18 @@ msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_opt
   return MSF_OK;
 }
 
+// The plain FP32 split-wave row pass's L2 prefetch ahead (MSF_ROW_L2AHEAD):
+// the distance in CTAs and, when the removed columns are not stored, only
+// the live element ranges of each row.
+static void set_row_ahead(const msf_context* ctx, const msf_specimen* spec, PassArgs* row) {
+  const int resident = row_split_resident_ctas(spec->g.ny);
+  row->l2_ahead = (int)((int64_t)resident * ctx->row_ahead_pct / 100);
+  const int ny = spec->g.ny;
+  const int whole[4] = {0, ny, ny, ny};
+  const int* r = row->row_dead_bits ? spec->row_live : whole;
+  for (int k = 0; k < 4; ++k) row->ahead_range[k] = r[k];
+}
+
 msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int reps,
                        double* ms_row, double* ms_col) {
   TraceScope trace_scope("time_passes");
@@ -557,6 +581,10 @@ msf_status time_passes(msf_context* ctx, const msf_specimen* spec, int nb, int r
     col.n_live_groups = spec->n_live_groups;
   }
   row.prefetch_tables = (pipe & MSF_ROW_PREFETCH) ? 1 : 0;
+  if (!fp64 && !staged_row && row_sched == 0 && !pipe_row && (pipe & MSF_ROW_L2AHEAD))
+    set_row_ahead(ctx, spec, &row);
+  row.lines_by_probe = (!fp64 && !staged_row && row_sched == 0 && !pipe_row &&
+                        (pipe & MSF_ROW_BYPROBE)) ? 1 : 0;
   PassArgs row_staged = row;  // schedule 1 reads the zero bits in its own layout
   if (row_sched == 1 && row.row_dead_bits) row_staged.row_dead_bits = spec->dead_bits_alt.as<uint32_t>();
   auto row_pass = [&]() {
@@ -1108,6 +1136,10 @@ msf_status raster_sums(msf_context* ctx, const RasterPlan& P, msf_results* res) 
   MSF_TRY(ctx->twiddles(g.nx, fp64, &col.tw));
   row.inv_s = col.inv_s = 1.0 / g.s;
   row.prefetch_tables = (!fp64 && (pipe & MSF_ROW_PREFETCH)) ? 1 : 0;
+  if (!fp64 && !staged_row && row_sched == 0 && !pipe_row && (pipe & MSF_ROW_L2AHEAD))
+    set_row_ahead(ctx, spec, &row);
+  row.lines_by_probe = (!fp64 && !staged_row && row_sched == 0 && !pipe_row &&
+                        (pipe & MSF_ROW_BYPROBE)) ? 1 : 0;
   row.probe = P.probe64.p;
   row.first_scale = g.nxny / g.s;
   col.mask_lo = spec->mask_lo.as<int32_t>();

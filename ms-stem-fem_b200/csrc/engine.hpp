@@ -77,8 +77,14 @@ constexpr int MSF_ROW_ALT = 8;
 // the plain split-wave row pass prefetches its transmission and vacuum rows
 // into L1 (PassArgs::prefetch_tables)
 constexpr int MSF_ROW_PREFETCH = 16;
-constexpr int MSF_PIPE_ALL =
-    MSF_PIPE_COL | MSF_PIPE_ROW | MSF_ROW_STAGED | MSF_ROW_ALT | MSF_ROW_PREFETCH;
+// the plain split-wave row pass (default schedule) prefetches the wavefield
+// rows of the CTAs one resident wave ahead into L2 (PassArgs::l2_ahead)
+constexpr int MSF_ROW_L2AHEAD = 32;
+// the plain split-wave row pass (default schedule) gives each CTA one row
+// of consecutive probes (PassArgs::lines_by_probe)
+constexpr int MSF_ROW_BYPROBE = 64;
+constexpr int MSF_PIPE_ALL = MSF_PIPE_COL | MSF_PIPE_ROW | MSF_ROW_STAGED | MSF_ROW_ALT |
+                             MSF_ROW_PREFETCH | MSF_ROW_L2AHEAD | MSF_ROW_BYPROBE;
 
 struct msf_context {
   int device = 0;
@@ -117,6 +123,9 @@ struct msf_context {
     return (pipe_env || it == tuned.end()) ? pipe : it->second.pipe;
   }
   bool pipe_env = false;  // MSF_PIPE given: it wins over tuning
+  // distance of the row pass's L2 prefetch (MSF_ROW_L2AHEAD) in percent of
+  // one resident wave of CTAs (MSF_ROW_AHEAD_PCT)
+  int row_ahead_pct = 100;
   // FEM ring bins per grid and dr (host sort of every pixel by k^2: 34 ms at
   // 1024^2, 180 ms at 2048^2), reused by every raster planned on that grid
   struct RingKey {
@@ -154,6 +163,10 @@ struct msf_specimen {
   std::vector<uint32_t> h_dead_bits;  // host copies (slot lanes compare them)
   std::vector<int32_t> h_live_groups;
   int n_live_groups = 0, n_live_columns = 0;
+  // element ranges of a row that hold live columns (two half-open ranges,
+  // even bounds; the whole row when no column is removed or the removed
+  // ones are not one run): what the row pass prefetches ahead into L2
+  int row_live[4] = {0, 0, 0, 0};
   msf::DevBuf kx, ky;         // FP64 domains for device set-up kernels
   std::vector<double> hprop;  // FP64 propagators, host copy
   std::vector<double> h_potential;  // [slice][nx][ny] complex, when kept

@@ -115,6 +115,31 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
+// PassArgs::l2_ahead: the first LINES threads of the CTA each issue bulk L2
+// prefetches of one wavefield row of the CTA a.l2_ahead places later in
+// launch order (grid (nb, nx / LINES), or (nb / LINES, nx) with the lines
+// by probe; x fastest).  Addresses and
+// sizes are multiples of 16 bytes: rows start at multiples of N complex
+// values and the ranges have even bounds.
+template <typename C, int N, int LINES>
+__device__ __forceinline__ void prefetch_rows_ahead(const PassArgs& a, bool by_probe) {
+  if (threadIdx.x >= LINES) return;
+  const int64_t lin = (int64_t)blockIdx.y * gridDim.x + blockIdx.x + a.l2_ahead;
+  if (lin >= (int64_t)gridDim.x * gridDim.y) return;
+  const int bx = (int)(lin % gridDim.x), by = (int)(lin / gridDim.x);
+  const int b = by_probe ? bx * LINES + (int)threadIdx.x : bx;
+  const int i = by_probe ? by : by * LINES + (int)threadIdx.x;
+  const C* row = static_cast<const C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)i * N;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int lo = a.ahead_range[2 * r], hi = a.ahead_range[2 * r + 1];
+    if (hi > lo)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                   ::"l"(row + lo), "r"((hi - lo) * (int)sizeof(C))
+                   : "memory");
+  }
+}
+
 // Split-wave transmission step (split_elem) on one row held in registers
 // (element t + T*m of row i); psi0 is the probe's vacuum wave, shifted like
 // the probe.
@@ -150,8 +175,11 @@ row_kernel(const PassArgs a) {
   C* smem = reinterpret_cast<C*>(smem_raw);
   const int line = threadIdx.x / T;
   const int t = threadIdx.x % T;
-  const int b = blockIdx.x;
-  const int i = blockIdx.y * LINES + line;
+  // lines of a CTA: consecutive rows of probe blockIdx.x, or row blockIdx.y
+  // of consecutive probes (PassArgs::lines_by_probe)
+  const bool by_probe = OP == ROW_SPLIT && a.lines_by_probe;
+  const int b = by_probe ? (int)blockIdx.x * LINES + line : (int)blockIdx.x;
+  const int i = by_probe ? (int)blockIdx.y : (int)blockIdx.y * LINES + line;
   C* sm = smem + line * SM::stride;
   C* row = static_cast<C*>(a.psi) + (int64_t)b * a.batch_stride + (int64_t)i * N;
   const C* tw = static_cast<const C*>(a.tw);
@@ -236,6 +264,8 @@ row_kernel(const PassArgs a) {
     // columns removed by the band limit were not stored: they are zero
     const uint32_t skip = (a.row_dead_bits && (a.row_dead_io & 1)) ? __ldg(a.row_dead_bits + t)
                                                                   : 0u;
+    if (OP == ROW_SPLIT && a.l2_ahead > 0)
+      prefetch_rows_ahead<C, N, LINES>(a, by_probe);
     if (OP == ROW_SPLIT && a.prefetch_tables) {
 #pragma unroll
       for (int m = 0; m < E; ++m)
@@ -402,6 +432,16 @@ cudaError_t row_launch(const PassArgs& a, cudaStream_t s) {
     int per = 1;
     while (per < 4 && groups % (2 * per) == 0 && groups / (2 * per) >= 256) per *= 2;
     groups /= per;
+  }
+  if (OP == ROW_SPLIT && a.lines_by_probe) {
+    if (a.nb % L == 0) {
+      k<<<dim3(a.nb / L, a.nx), L * Sh::T, smem, s>>>(a);
+      return cudaGetLastError();
+    }
+    PassArgs rows = a;  // a batch the lines do not divide: rows of one probe
+    rows.lines_by_probe = 0;
+    k<<<dim3(a.nb, groups), L * Sh::T, smem, s>>>(rows);
+    return cudaGetLastError();
   }
   dim3 grid(a.nb, groups);
   k<<<grid, L * Sh::T, smem, s>>>(a);
@@ -970,6 +1010,42 @@ int sm_count() {
     if (dev >= 0 && dev < 64) cached[dev].store(n);
   }
   return n;
+}
+
+namespace {
+template <int N>
+int row_split_resident(int dev) {
+  // per device: the occupancy query does not change within a process
+  static std::atomic<int> cached[64];
+  int n = (dev >= 0 && dev < 64) ? cached[dev].load() : 0;
+  if (n > 0) return n;
+  constexpr int L = row_lines<float, N, 0>();
+  using Sh = Shape<N, float, 0>;
+  constexpr int smem = L * Smem<Sh, 8, L, false>::stride * 8;
+  static PerDevice configured;
+  auto k = row_kernel<float, N, L, ROW_SPLIT, 0>;
+  int per_sm = 0;
+  if (smem_limit_once((const void*)k, smem, configured) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, L * Sh::T, smem) != cudaSuccess)
+    return 0;
+  n = per_sm * sm_count();
+  if (n > 0 && dev >= 0 && dev < 64) cached[dev].store(n);
+  return n;
+}
+}  // namespace
+
+int row_split_resident_ctas(int ny) {
+  const int dev = current_device();
+  switch (ny) {
+    case 64: return row_split_resident<64>(dev);
+    case 128: return row_split_resident<128>(dev);
+    case 256: return row_split_resident<256>(dev);
+    case 512: return row_split_resident<512>(dev);
+    case 1024: return row_split_resident<1024>(dev);
+    case 2048: return row_split_resident<2048>(dev);
+    case 4096: return row_split_resident<4096>(dev);
+  }
+  return 0;
 }
 
 bool supported_length(int n) {

@@ -125,6 +125,21 @@ struct PassArgs {
   // wavefield past L1, so the update after the inverse transform finds its
   // tables in L1
   int prefetch_tables = 0;
+  // split-wave row pass (ROW_SPLIT, plain launch): each CTA bulk-prefetches
+  // into L2 the wavefield rows of the CTA l2_ahead places later in launch
+  // order (0: off).  CTAs start in increasing linear order, so with
+  // l2_ahead about one resident wave that CTA starts as this one ends and
+  // finds its rows in L2 instead of waiting on HBM.  Only the element
+  // ranges [ahead_range[0], ahead_range[1]) and [ahead_range[2],
+  // ahead_range[3]) of a row are fetched (the live columns; even bounds).
+  int l2_ahead = 0;
+  int ahead_range[4] = {0, 0, 0, 0};
+  // split-wave row pass (ROW_SPLIT, plain launch): the lines of a CTA are
+  // one row of consecutive probes (grid (nb / lines, nx)) instead of
+  // consecutive rows of one probe, so they share the row's transmission
+  // and, for probes of one raster line, its vacuum row in L1.  Ignored when
+  // nb is not a multiple of the lines per CTA.
+  int lines_by_probe = 0;
 };
 
 // Vacuum part of the exit wave for split-wave detection: k-space values of
@@ -144,6 +159,10 @@ int row_line_threads(int n, bool fp64);
 // Columns per tile of the pipelined column pass (0 if unsupported).
 int pipe_cols_for(int nx, bool fp64);
 cudaError_t launch_row(bool fp64, RowOp op, const PassArgs& a, cudaStream_t s);
+// CTAs of the FP32 split-wave row pass (ROW_SPLIT, default schedule) that
+// the current device holds at once for rows of length ny (0 if
+// unsupported): the natural PassArgs::l2_ahead.
+int row_split_resident_ctas(int ny);
 // The FP32 split-wave row pass (ROW_SPLIT) on the alternative FFT radix
 // schedule (16 elements a thread from 512 points, 8 at 256; row_dead_bits
 // in that schedule's layout, staged_row_threads(ny, 1)); row lengths

@@ -53,11 +53,20 @@ msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
   if (!ctx->pipe_env) {
     const bool col = pipe_supported(g.nx, g.ny, ctx->fp64);
     const bool staged = !ctx->fp64 && staged_row_supported(g.nx, g.ny);
-    // column pass plain or pipelined; FP32 row pass plain or staged, each
-    // on either FFT radix schedule
+    // column pass plain or pipelined; FP32 row pass plain (with or without
+    // its L1 table and L2 wavefield prefetches, lines by row or by probe)
+    // or staged, each on either FFT radix schedule
     std::vector<int> rows{0};
     if (staged)
-      rows = {0, MSF_ROW_PREFETCH, MSF_ROW_ALT, MSF_ROW_STAGED, MSF_ROW_STAGED | MSF_ROW_ALT};
+      rows = {0,
+              MSF_ROW_PREFETCH,
+              MSF_ROW_L2AHEAD,
+              MSF_ROW_PREFETCH | MSF_ROW_L2AHEAD,
+              MSF_ROW_PREFETCH | MSF_ROW_BYPROBE,
+              MSF_ROW_PREFETCH | MSF_ROW_L2AHEAD | MSF_ROW_BYPROBE,
+              MSF_ROW_ALT,
+              MSF_ROW_STAGED,
+              MSF_ROW_STAGED | MSF_ROW_ALT};
     pipes.clear();
     for (int c : col ? std::vector<int>{0, MSF_PIPE_COL} : std::vector<int>{0})
       for (int r : rows) pipes.push_back(c | r);
