@@ -518,7 +518,7 @@ msf_status build_probe(msf_context* ctx, const msf_specimen* spec, const msf_opt
 // The plain FP32 split-wave row pass's L2 prefetch ahead (MSF_ROW_L2AHEAD):
 // the distance in CTAs and, when the removed columns are not stored, only
 // the live element ranges of each row.
-static void set_row_ahead(const msf_context* ctx, const msf_specimen* spec, PassArgs* row) {
+void set_row_ahead(const msf_context* ctx, const msf_specimen* spec, PassArgs* row) {
   const int resident = row_split_resident_ctas(spec->g.ny);
   row->l2_ahead = (int)((int64_t)resident * ctx->row_ahead_pct / 100);
   const int ny = spec->g.ny;

@@ -257,6 +257,10 @@ msf_status run_batch(msf_context* ctx, int n, const msf_specimen* const* specs,
                      const msf_optics* optics, const msf_raster* rasters,
                      const msf_detect* detects, msf_results* results, int slots);
 int lane_slots(int want, int64_t plane, int lanes, int64_t probes);
+struct PassArgs;
+// The plain FP32 split-wave row pass's L2 prefetch ahead (MSF_ROW_L2AHEAD)
+// for rows of `spec`'s grid: distance and live element ranges.
+void set_row_ahead(const msf_context* ctx, const msf_specimen* spec, PassArgs* row);
 struct SplitK;
 // The detector MTF stage of nb exit waves into FP64 planes `out` (the plan
 // supplies the grid, aperture and the 2-D MTF).

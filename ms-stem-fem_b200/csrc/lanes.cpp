@@ -2,6 +2,7 @@
 #include "lanes.hpp"
 
 #include <algorithm>
+#include <cstdlib>
 #include <string>
 
 namespace msf {
@@ -60,8 +61,9 @@ msf_status Lane::init() {
   MSF_TRY(ctx_->alloc(&psi_, 8 * (size_t)plane_ * B_));
   // idle slots are still read by the column pass's tile copies
   MSF_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, stream_));
-  table_bytes_ = round_up(sizeof(SlotPass) * B_ + sizeof(DetectTable) +
-                              sizeof(DetectSlot) * B_, 256);
+  shift_off_ = round_up(sizeof(SlotPass) * B_ + sizeof(DetectTable) +
+                            sizeof(DetectSlot) * B_, 256);
+  table_bytes_ = round_up(shift_off_ + sizeof(int32_t) * 2 * B_, 256);
   MSF_TRY(ctx_->alloc(&table_, table_bytes_));
   MSF_CUDA(cudaMemsetAsync(table_.p, 0, table_bytes_, stream_));
   MSF_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&host_ring_), kRing * table_bytes_,
@@ -70,6 +72,10 @@ msf_status Lane::init() {
   MSF_TRY(ctx_->alloc(&err_, sizeof(int)));
   MSF_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
   pipe_col_ = (ctx_->pipe & MSF_PIPE_COL) && pipe_supported(nx_, ny_);
+  // MSF_LANE_UNIFORM=0: every step runs the slot passes (the two paths give
+  // the same bits; the switch lets tests and benchmarks compare them)
+  const char* u = std::getenv("MSF_LANE_UNIFORM");
+  uniform_ok_ = !(u && u[0] == '0');
   if (pipe_col_) MSF_CUDA(encode_column_map(psi_.p, B_, nx_, ny_, col_map_));
   row_.psi = col_.psi = psi_.p;
   row_.batch_stride = col_.batch_stride = plane_;
@@ -168,6 +174,45 @@ msf_status Lane::launch_passes() {
   return MSF_OK;
 }
 
+msf_status Lane::launch_uniform(const SlotJob* job, int s, int nb) {
+  const RasterPlan& P = job->plan;
+  const msf_specimen* spec = P.spec;
+  const bool last = s + 1 == P.S;
+  // the lane's pass arguments (buffer, twiddles, removed columns) for the
+  // first nb wavefields, with this slice's tables, as msf_run sets them
+  PassArgs row = row_, col = col_;
+  row.slots = col.slots = nullptr;
+  row.nb = col.nb = nb;
+  row.shifts = reinterpret_cast<const int32_t*>(static_cast<const char*>(table_.p) +
+                                                shift_off_);
+  row.trans = static_cast<const char*>(spec->t.p) + 8 * plane_ * s;
+  row.psi0 = static_cast<const char*>(P.psi0_tab.p) + 8 * plane_ * s;
+  // removed columns: read as zero after the first slice, stored (as zeros)
+  // only at the last
+  row.row_dead_io = row.row_dead_bits ? ((s > 0 ? 1 : 0) | (last ? 0 : 2)) : 0;
+  // the tuned row variants that round as the slot pass does (the default
+  // FFT schedule): L1 table prefetch, L2 row prefetch, lines by probe, staged
+  const int pipe = ctx_->pipe_for(nx_, ny_);
+  const bool staged = staged_row_supported(nx_, ny_) && (pipe & MSF_ROW_STAGED);
+  row.prefetch_tables = (pipe & MSF_ROW_PREFETCH) ? 1 : 0;
+  row.l2_ahead = 0;
+  if (!staged && (pipe & MSF_ROW_L2AHEAD)) set_row_ahead(ctx_, spec, &row);
+  row.lines_by_probe = (!staged && (pipe & MSF_ROW_BYPROBE)) ? 1 : 0;
+  if (s > 0 && staged)
+    MSF_CUDA(launch_row_split_staged(row, err_.as<int>(), stream_, 0));
+  else
+    MSF_CUDA(launch_row(false, s == 0 ? ROW_SPLIT_FIRST : ROW_SPLIT, row, stream_));
+  col.px = static_cast<const char*>(spec->prop.p) + 8 * (size_t)(nx_ + ny_) * s;
+  col.py = static_cast<const char*>(col.px) + 8 * (size_t)nx_;
+  col.mask_lo = spec->mask_lo.as<int32_t>();
+  col.mask_hi = spec->mask_hi.as<int32_t>();
+  if (pipe_col_)
+    MSF_CUDA(launch_col_slice_pipe(col, last, col_map_, err_.as<int>(), stream_));
+  else
+    MSF_CUDA(launch_col(false, last ? COL_SLICE_LAST : COL_SLICE, col, stream_));
+  return MSF_OK;
+}
+
 msf_status Lane::launch_detect() {
   const char* det = static_cast<const char*>(table_.p) + sizeof(SlotPass) * B_;
   MSF_CUDA(launch_slot_detect(det, B_, max_chunks_, nx_, ny_, partial_.as<double>(), true,
@@ -226,10 +271,22 @@ msf_status Lane::step() {
   DetectTable* dt = reinterpret_cast<DetectTable*>(h + sizeof(SlotPass) * B_);
   DetectSlot* de = reinterpret_cast<DetectSlot*>(dt + 1);
   std::vector<int> done;
+  int32_t* hshift = reinterpret_cast<int32_t*>(h + shift_off_);
+  // uniform step: the active slots are 0..n_act-1, all at slice uni_s of
+  // raster uni_job
+  const SlotJob* uni_job = nullptr;
+  int uni_s = -1, n_act = 0;
+  bool uniform = true;
   for (int i = 0; i < B_; ++i) {
     const Slot& sl = slot_[i];
     SlotPass p;
     if (sl.job) {
+      if (i != n_act || (uni_job && (sl.job != uni_job || sl.s != uni_s))) uniform = false;
+      uni_job = sl.job;
+      uni_s = sl.s;
+      ++n_act;
+      hshift[2 * i] = sl.job->plan.shifts[2 * sl.probe];
+      hshift[2 * i + 1] = sl.job->plan.shifts[2 * sl.probe + 1];
       const RasterPlan& P = sl.job->plan;
       const msf_specimen* spec = P.spec;
       p.op = sl.s == 0 ? SLOT_FIRST : SLOT_NEXT;
@@ -279,20 +336,29 @@ msf_status Lane::step() {
     de[k] = e;
   }
   *dt = t;
-  // the slot part always; the detection part when some slot finishes
+  uniform = uniform && uniform_ok_ && n_act > 0;
+  // the slot part always; the detection part when some slot finishes; the
+  // shifts on uniform steps
   const size_t pass_bytes = sizeof(SlotPass) * B_;
   const size_t det_bytes = t.n_done ? sizeof(DetectTable) + sizeof(DetectSlot) * t.n_done : 0;
-  MSF_CUDA(cudaMemcpyAsync(table_.p, h, pass_bytes + det_bytes, cudaMemcpyHostToDevice,
-                           stream_));
+  const size_t copy_bytes = uniform ? shift_off_ + sizeof(int32_t) * 2 * n_act
+                                    : pass_bytes + det_bytes;
+  MSF_CUDA(cudaMemcpyAsync(table_.p, h, copy_bytes, cudaMemcpyHostToDevice, stream_));
   MSF_CUDA(cudaEventRecord(ring_ev_[r], stream_));
 
-  // the first step runs its launches directly (kernel attributes are set
-  // on first use); later steps replay the captured graphs
-  if (ctx_->graphs && steps_ >= 1 && !graph_pass_) MSF_TRY(capture_passes());
-  if (graph_pass_) {
-    MSF_CUDA(cudaGraphLaunch(graph_pass_, stream_));
+  if (uniform) {
+    MSF_TRY(launch_uniform(uni_job, uni_s, n_act));
+    ++uniform_steps_;
   } else {
-    MSF_TRY(launch_passes());
+    // the first slot step runs its launches directly (kernel attributes
+    // are set on first use); later ones replay the captured graph
+    if (ctx_->graphs && slot_steps_ >= 1 && !graph_pass_) MSF_TRY(capture_passes());
+    if (graph_pass_) {
+      MSF_CUDA(cudaGraphLaunch(graph_pass_, stream_));
+    } else {
+      MSF_TRY(launch_passes());
+    }
+    ++slot_steps_;
   }
   launches_ += 2;
   if (t.n_done) {

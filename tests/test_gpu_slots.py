@@ -73,6 +73,27 @@ def test_batch_matches_single_runs(slots):
         assert_same_run(o, r, 1e-6, 1e-9, "job %d slots %d" % (k, slots))
 
 
+@pytest.mark.parametrize("slots", [4, 9])
+def test_uniform_steps_match_slot_passes(slots, monkeypatch):
+    """A step whose active slots all hold one raster's probes at one slice
+    runs the batched passes of msf_run; with MSF_LANE_UNIFORM=0 every step
+    runs the slot passes.  Both give the same bits (4 slots: the 36-probe
+    raster fills the lane in whole groups; 9: groups end part-filled and
+    rasters share steps)."""
+    ctx = msf.Context(precision="fp32")
+    js = jobs_mixed()
+    specs = [ctx.specimen(j.grid, j.pos, j.z) for j in js]
+    batch = [(s, j.optics, j.raster, j.detect) for s, j in zip(specs, js)]
+    monkeypatch.setenv("MSF_LANE_UNIFORM", "0")
+    slot_only = ctx.run_batch(batch, slots=slots)
+    monkeypatch.setenv("MSF_LANE_UNIFORM", "1")
+    mixed = ctx.run_batch(batch, slots=slots)
+    for k, (a, b) in enumerate(zip(mixed, slot_only)):
+        assert np.array_equal(a.adf_image, b.adf_image), k
+        for mode in b.v:
+            assert np.array_equal(a.v[mode], b.v[mode], equal_nan=True), (k, mode)
+
+
 def test_batch_rejects_fp64_context():
     ctx = msf.Context(precision="fp64")
     j = jobs_mixed()[1]
