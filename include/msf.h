@@ -232,12 +232,12 @@ msf_status msf_probe(msf_context* ctx, const msf_specimen* spec,
  * For callers that may not call cudaMalloc (an application that owns all
  * device memory in its own pool, a running loop that must not stall on an
  * allocation).  Its scratch is one fixed device array per device, sized for
- * grids of at most 2048 x 2048; larger grids return MSF_ERR_ARG.  A call
- * that is not being captured looks up that array's address (again on every
- * such call, so a device reset leaves nothing stale); a captured call uses
- * the address of the last uncaptured call on its device, so one uncaptured
- * call must come first.  Calls that overlap on the GPU share the array and
- * race. */
+ * grids of at most 2048 x 2048; larger grids return MSF_ERR_ARG.  The first
+ * call on a device looks up that array's address (cudaGetSymbolAddress,
+ * with the device current), and so does every later call made outside a
+ * stream capture (a device reset then leaves nothing stale): make the first
+ * call on each device before any stream capture.  Calls that overlap on the
+ * GPU share the array and race. */
 msf_status msf_probe_noalloc(const msf_grid* grid, const msf_optics* optics,
                              double* probe_device, void* stream);
 

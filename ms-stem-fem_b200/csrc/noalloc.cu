@@ -10,11 +10,10 @@
 // device array, sized for grids of at most kMaxSide x kMaxSide.
 //
 // Behaviour a caller must know:
-//  * A call that is not being captured looks up the array's device address
-//    (cudaGetSymbolAddress) with its device current, every time; a call
-//    inside a stream capture uses the address of the last uncaptured call
-//    on that device, so make one call before any capture (and again after
-//    a cudaDeviceReset, before capturing).
+//  * The first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress) with that device current, and so does every
+//    later call made outside a stream capture; make the first call on each
+//    device before any stream capture (and again after a cudaDeviceReset).
 //  * The probe equals msf_probe's to within FP64 rounding (1e-12 of its
 //    largest value), not bit for bit: the twiddles here come from the
 //    device's sincospi, msf_probe's from host cos/sin.
@@ -55,9 +54,8 @@ void* g_address[kMaxDevices] = {};
 // Device address of the scratch array on the current device.  Outside a
 // stream capture it is looked up again on every call (a host-side query
 // that allocates nothing), so a context the application tore down and
-// recreated (cudaDeviceReset) cannot leave a stale address behind; while
-// the stream is capturing, the address of the last uncaptured call on this
-// device is used, so such a call must come first.
+// recreated (cudaDeviceReset) cannot leave a stale address behind; the
+// first call on a device must therefore not be inside a capture.
 msf_status scratch_address(int device, cudaStream_t s, unsigned char** out) {
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
