@@ -77,23 +77,28 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(which, nb):
+def ncu_traffic(which, nb, pipe=None):
     """DRAM bytes per launch of the row or column pass ("row" / "col") at nb
     probes per launch, from the committed ncu summaries (profiles/*.md): a
-    figure captured at nb itself when one exists, else the 32-probe capture
-    scaled by nb / 32 (DRAM bytes grow in proportion to the probes a launch
-    carries).  Returns (bytes, how) or (None, None)."""
+    figure captured at nb with the same slice-pass variants (`pipe`, the
+    tuner's mask) when one exists, else one captured at nb, else the
+    32-probe capture scaled by nb / 32 (DRAM bytes grow in proportion to the
+    probes a launch carries).  Returns (bytes, how) or (None, None)."""
+    same = "traffic_bytes_per_launch_%s_b%d_pipe%s:" % (which, nb, pipe)
     exact = "traffic_bytes_per_launch_%s_b%d:" % (which, nb)
     base = "traffic_bytes_per_launch_%s:" % which
     found = {}
     for p in sorted((ROOT / "profiles").glob("*.md")):
         for line in p.read_text().splitlines():
-            for key in (exact, base):
+            for key in (same, exact, base):
                 if line.startswith(key) and key not in found:
                     try:
                         found[key] = (float(line.split(":", 1)[1].split()[0]), p.name)
                     except ValueError:
                         pass
+    if pipe is not None and same in found:
+        return found[same][0], ("ncu capture at %d probes per launch, slice-pass variants %s "
+                                "(%s)" % (nb, pipe, found[same][1]))
     if exact in found:
         return found[exact][0], "ncu capture at %d probes per launch (%s)" % (nb, found[exact][1])
     if base in found:
@@ -675,8 +680,9 @@ def main():
     t_dom = max(ms_row, ms_col) * 1e-3
     peak, peak_kind = measured_peaks()
     achieved = alg / t_dom / 1e9
-    traffic, traffic_src = (ncu_traffic(dom, nb) if (n == 1024 and args.precision == "fp32")
-                            else (None, None))
+    pipe_used = tuning["pipe"] if tuning else int(os.environ.get("MSF_PIPE", "17"))
+    traffic, traffic_src = (ncu_traffic(dom, nb, pipe_used)
+                            if (n == 1024 and args.precision == "fp32") else (None, None))
     # the flop ceiling beside the HBM one: two complex 2-D FFTs at
     # 5 n log2 n plus the point-wise work, per probe*slice, against the
     # FP32 CUDA-core peak (SMs x 128 lanes x 2 flops x max SM clock;
