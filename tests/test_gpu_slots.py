@@ -94,6 +94,41 @@ def test_uniform_steps_match_slot_passes(slots, monkeypatch):
             assert np.array_equal(a.v[mode], b.v[mode], equal_nan=True), (k, mode)
 
 
+class LargeJob(JobSpec):
+    """A thin seeded slab on a 1024^2 or 2048^2 grid (positions from the
+    library's generator, which is fast at these atom counts)."""
+
+    def __init__(self, n, zbox, seed, raster_n):
+        box = n * 0.09766
+        super().__init__(n, box, zbox, 1, seed, raster_n)
+        self.pos = msf.amorphous_positions(int(0.05 * box * box * zbox), (box, box, zbox), 2.2,
+                                           seed=seed)
+        self.z = np.full(len(self.pos), 14, dtype=np.uint32)
+
+
+def test_large_grid_lanes_match_single_runs(monkeypatch):
+    """The slot passes and the batched passes of the lanes at the 1024- and
+    2048-point shapes (thin slabs, 3 slices; 7 slots, so the 25- and 9-probe
+    rasters leave part-filled groups and mix): each raster matches its own
+    msf_run, and the uniform steps give the same bits as slot passes only."""
+    js = [LargeJob(1024, 6.0, 71, 5), LargeJob(2048, 6.0, 72, 3),
+          LargeJob(1024, 6.0, 73, 3), LargeJob(2048, 6.0, 74, 3)]
+    ctx = msf.Context(precision="fp32", batch=8)
+    specs = [ctx.specimen(j.grid, j.pos, j.z) for j in js]
+    batch = [(s, j.optics, j.raster, j.detect) for s, j in zip(specs, js)]
+    singles = [ctx.run(*b) for b in batch]
+    outs = ctx.run_batch(batch, slots=7)
+    for k, (o, r) in enumerate(zip(outs, singles)):
+        assert o.probe_slices == r.probe_slices
+        assert_same_run(o, r, 1e-6, 1e-9, "large job %d" % k)
+    monkeypatch.setenv("MSF_LANE_UNIFORM", "0")
+    slot_only = ctx.run_batch(batch, slots=7)
+    for k, (a, b) in enumerate(zip(outs, slot_only)):
+        assert np.array_equal(a.adf_image, b.adf_image), k
+        for mode in b.v:
+            assert np.array_equal(a.v[mode], b.v[mode], equal_nan=True), (k, mode)
+
+
 def test_batch_rejects_fp64_context():
     ctx = msf.Context(precision="fp64")
     j = jobs_mixed()[1]
