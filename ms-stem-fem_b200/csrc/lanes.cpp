@@ -72,10 +72,10 @@ msf_status Lane::init() {
   MSF_TRY(ctx_->alloc(&err_, sizeof(int)));
   MSF_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
   pipe_col_ = (ctx_->pipe & MSF_PIPE_COL) && pipe_supported(nx_, ny_);
-  // MSF_LANE_UNIFORM=0: every step runs the slot passes (the two paths give
+  // MSF_LANE_GROUPS=0: every step runs the slot passes (the two paths give
   // the same bits; the switch lets tests and benchmarks compare them)
-  const char* u = std::getenv("MSF_LANE_UNIFORM");
-  uniform_ok_ = !(u && u[0] == '0');
+  const char* u = std::getenv("MSF_LANE_GROUPS");
+  groups_ok_ = !(u && u[0] == '0');
   if (pipe_col_) MSF_CUDA(encode_column_map(psi_.p, B_, nx_, ny_, col_map_));
   row_.psi = col_.psi = psi_.p;
   row_.batch_stride = col_.batch_stride = plane_;
@@ -174,17 +174,18 @@ msf_status Lane::launch_passes() {
   return MSF_OK;
 }
 
-msf_status Lane::launch_uniform(const SlotJob* job, int s, int nb) {
+msf_status Lane::launch_group(const SlotJob* job, int s, int base, int nb) {
   const RasterPlan& P = job->plan;
   const msf_specimen* spec = P.spec;
   const bool last = s + 1 == P.S;
-  // the lane's pass arguments (buffer, twiddles, removed columns) for the
-  // first nb wavefields, with this slice's tables, as msf_run sets them
+  // the lane's pass arguments (twiddles, removed columns) for wavefields
+  // base .. base + nb - 1, with this slice's tables, as msf_run sets them
   PassArgs row = row_, col = col_;
   row.slots = col.slots = nullptr;
+  row.psi = col.psi = static_cast<char*>(psi_.p) + 8 * plane_ * base;
   row.nb = col.nb = nb;
   row.shifts = reinterpret_cast<const int32_t*>(static_cast<const char*>(table_.p) +
-                                                shift_off_);
+                                                shift_off_) + 2 * base;
   row.trans = static_cast<const char*>(spec->t.p) + 8 * plane_ * s;
   row.psi0 = static_cast<const char*>(P.psi0_tab.p) + 8 * plane_ * s;
   // removed columns: read as zero after the first slice, stored (as zeros)
@@ -206,10 +207,19 @@ msf_status Lane::launch_uniform(const SlotJob* job, int s, int nb) {
   col.py = static_cast<const char*>(col.px) + 8 * (size_t)nx_;
   col.mask_lo = spec->mask_lo.as<int32_t>();
   col.mask_hi = spec->mask_hi.as<int32_t>();
-  if (pipe_col_)
-    MSF_CUDA(launch_col_slice_pipe(col, last, col_map_, err_.as<int>(), stream_));
-  else
+  if (pipe_col_) {
+    // the lane's tensor map starts at wavefield 0; a group further in gets
+    // its own (encoding is a host call that allocates nothing)
+    alignas(64) unsigned char map[128];
+    const void* m = col_map_;
+    if (base != 0) {
+      MSF_CUDA(encode_column_map(col.psi, nb, nx_, ny_, map));
+      m = map;
+    }
+    MSF_CUDA(launch_col_slice_pipe(col, last, m, err_.as<int>(), stream_));
+  } else {
     MSF_CUDA(launch_col(false, last ? COL_SLICE_LAST : COL_SLICE, col, stream_));
+  }
   return MSF_OK;
 }
 
@@ -246,20 +256,31 @@ msf_status Lane::capture_detect() {
 
 msf_status Lane::step() {
   if (!busy()) return MSF_OK;
-  // refill idle slots from the queue: oldest raster first, or (fair) the
-  // raster with the fewest probes in flight
-  for (int i = 0; i < B_ && !queue_.empty(); ++i) {
-    if (slot_[i].job) continue;
+  // refill idle slots, in slot order, from the queue: oldest raster first,
+  // or (fair) the raster with the fewest probes in flight, which takes a
+  // contiguous share of the idle slots (ceil(idle left / rasters waiting),
+  // at most its waiting probes; then the choice is made again), so that a
+  // raster's probes sit in neighbouring slots and can run as one group
+  std::vector<int> idle;
+  for (int i = 0; i < B_; ++i)
+    if (!slot_[i].job) idle.push_back(i);
+  for (size_t k = 0; k < idle.size() && !queue_.empty();) {
     auto pick = queue_.begin();
     if (fair_)
       for (auto it = queue_.begin(); it != queue_.end(); ++it)
         if ((*it)->started - (*it)->done < (*pick)->started - (*pick)->done) pick = it;
     SlotJob* j = *pick;
-    slot_[i].job = j;
-    slot_[i].probe = j->next_probe++;
-    slot_[i].s = 0;
-    ++j->started;
-    ++active_;
+    const size_t left = idle.size() - k;
+    int64_t take = fair_ ? (int64_t)((left + queue_.size() - 1) / queue_.size()) : (int64_t)left;
+    take = std::min<int64_t>(take, j->plan.n_probes - j->next_probe);
+    for (int64_t q = 0; q < take; ++q) {
+      Slot& sl = slot_[idle[k++]];
+      sl.job = j;
+      sl.probe = j->next_probe++;
+      sl.s = 0;
+      ++j->started;
+      ++active_;
+    }
     if (j->next_probe == j->plan.n_probes) queue_.erase(pick);
   }
 
@@ -272,19 +293,21 @@ msf_status Lane::step() {
   DetectSlot* de = reinterpret_cast<DetectSlot*>(dt + 1);
   std::vector<int> done;
   int32_t* hshift = reinterpret_cast<int32_t*>(h + shift_off_);
-  // uniform step: the active slots are 0..n_act-1, all at slice uni_s of
-  // raster uni_job
-  const SlotJob* uni_job = nullptr;
-  int uni_s = -1, n_act = 0;
-  bool uniform = true;
+  // groups: runs of neighbouring active slots at one slice of one raster
+  struct Group {
+    const SlotJob* job;
+    int s, base, nb;
+  };
+  std::vector<Group> groups;
   for (int i = 0; i < B_; ++i) {
     const Slot& sl = slot_[i];
     SlotPass p;
     if (sl.job) {
-      if (i != n_act || (uni_job && (sl.job != uni_job || sl.s != uni_s))) uniform = false;
-      uni_job = sl.job;
-      uni_s = sl.s;
-      ++n_act;
+      Group* g = groups.empty() ? nullptr : &groups.back();
+      if (g && g->base + g->nb == i && g->job == sl.job && g->s == sl.s)
+        ++g->nb;
+      else
+        groups.push_back(Group{sl.job, sl.s, i, 1});
       hshift[2 * i] = sl.job->plan.shifts[2 * sl.probe];
       hshift[2 * i + 1] = sl.job->plan.shifts[2 * sl.probe + 1];
       const RasterPlan& P = sl.job->plan;
@@ -336,19 +359,22 @@ msf_status Lane::step() {
     de[k] = e;
   }
   *dt = t;
-  uniform = uniform && uniform_ok_ && n_act > 0;
+  // a step of at most kMaxGroups groups runs each group through the batched
+  // passes; more fragmented steps run the slot passes
+  const bool grouped = groups_ok_ && !groups.empty() && (int)groups.size() <= kMaxGroups;
   // the slot part always; the detection part when some slot finishes; the
-  // shifts on uniform steps
+  // shifts on grouped steps
   const size_t pass_bytes = sizeof(SlotPass) * B_;
   const size_t det_bytes = t.n_done ? sizeof(DetectTable) + sizeof(DetectSlot) * t.n_done : 0;
-  const size_t copy_bytes = uniform ? shift_off_ + sizeof(int32_t) * 2 * n_act
+  const size_t copy_bytes = grouped ? shift_off_ + sizeof(int32_t) * 2 * B_
                                     : pass_bytes + det_bytes;
   MSF_CUDA(cudaMemcpyAsync(table_.p, h, copy_bytes, cudaMemcpyHostToDevice, stream_));
   MSF_CUDA(cudaEventRecord(ring_ev_[r], stream_));
 
-  if (uniform) {
-    MSF_TRY(launch_uniform(uni_job, uni_s, n_act));
-    ++uniform_steps_;
+  if (grouped) {
+    for (const Group& g : groups) MSF_TRY(launch_group(g.job, g.s, g.base, g.nb));
+    launches_ += 2 * ((int64_t)groups.size() - 1);
+    ++grouped_steps_;
   } else {
     // the first slot step runs its launches directly (kernel attributes
     // are set on first use); later ones replay the captured graph

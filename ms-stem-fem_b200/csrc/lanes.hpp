@@ -13,12 +13,14 @@
 // once as two CUDA graphs (the passes; the detection, replayed only on steps
 // where some slot finishes) and replayed.
 //
-// A step whose active slots are slots 0..n-1 and all hold probes of one
-// raster at one slice (a raster with at least as many waiting probes as
-// the lane has slots fills the lane that way, and its probes then advance
-// together) runs the batched passes of msf_run over those n wavefields
-// instead, with the probes' shifts from the step's table: the same
-// arithmetic (bit-identical) without the per-slot table reads.
+// The active slots of a step fall into groups: runs of neighbouring slots
+// whose probes belong to one raster and are at one slice (probes that
+// start together advance together, and refills hand each raster a
+// contiguous run of slots).  A step of at most kMaxGroups groups runs each
+// group through the batched passes of msf_run over its wavefields, with
+// the probes' shifts from the step's table: the same arithmetic
+// (bit-identical) without the per-slot table reads.  Steps more fragmented
+// than that run the slot passes.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -79,9 +81,8 @@ class Lane {
   int slots() const { return B_; }
   int64_t steps() const { return steps_; }
   int64_t launches() const { return launches_; }
-  // steps that ran the batched passes (every active slot at one slice of
-  // one raster)
-  int64_t uniform_steps() const { return uniform_steps_; }
+  // steps that ran the batched passes per group of slots
+  int64_t grouped_steps() const { return grouped_steps_; }
 
  private:
   struct Slot {
@@ -92,7 +93,7 @@ class Lane {
   msf_status capture_passes();
   msf_status capture_detect();
   msf_status launch_passes();
-  msf_status launch_uniform(const SlotJob* job, int s, int nb);
+  msf_status launch_group(const SlotJob* job, int s, int base, int nb);
   msf_status launch_detect();
   msf_status grow_chunks(int n_chunks);
 
@@ -115,8 +116,9 @@ class Lane {
   PassArgs row_, col_;
   size_t table_bytes_ = 0;
   size_t shift_off_ = 0;  // [B][2] int32 probe shifts after the detection part
-  int64_t uniform_steps_ = 0, slot_steps_ = 0;
-  bool uniform_ok_ = true;
+  int64_t grouped_steps_ = 0, slot_steps_ = 0;
+  static constexpr int kMaxGroups = 8;
+  bool groups_ok_ = true;
   static constexpr int kRing = 4;
   unsigned char* host_ring_ = nullptr;  // kRing pinned tables
   cudaEvent_t ring_ev_[kRing] = {};

@@ -74,19 +74,19 @@ def test_batch_matches_single_runs(slots):
 
 
 @pytest.mark.parametrize("slots", [4, 9])
-def test_uniform_steps_match_slot_passes(slots, monkeypatch):
-    """A step whose active slots all hold one raster's probes at one slice
-    runs the batched passes of msf_run; with MSF_LANE_UNIFORM=0 every step
-    runs the slot passes.  Both give the same bits (4 slots: the 36-probe
-    raster fills the lane in whole groups; 9: groups end part-filled and
-    rasters share steps)."""
+def test_grouped_steps_match_slot_passes(slots, monkeypatch):
+    """Runs of neighbouring slots holding one raster's probes at one slice
+    go through the batched passes of msf_run, one launch pair per run; with
+    MSF_LANE_GROUPS=0 every step runs the slot passes.  Both give the same
+    bits (4 slots: the 36-probe raster fills the lane in whole groups; 9:
+    groups end part-filled and rasters share steps in several runs)."""
     ctx = msf.Context(precision="fp32")
     js = jobs_mixed()
     specs = [ctx.specimen(j.grid, j.pos, j.z) for j in js]
     batch = [(s, j.optics, j.raster, j.detect) for s, j in zip(specs, js)]
-    monkeypatch.setenv("MSF_LANE_UNIFORM", "0")
+    monkeypatch.setenv("MSF_LANE_GROUPS", "0")
     slot_only = ctx.run_batch(batch, slots=slots)
-    monkeypatch.setenv("MSF_LANE_UNIFORM", "1")
+    monkeypatch.setenv("MSF_LANE_GROUPS", "1")
     mixed = ctx.run_batch(batch, slots=slots)
     for k, (a, b) in enumerate(zip(mixed, slot_only)):
         assert np.array_equal(a.adf_image, b.adf_image), k
@@ -110,7 +110,7 @@ def test_large_grid_lanes_match_single_runs(monkeypatch):
     """The slot passes and the batched passes of the lanes at the 1024- and
     2048-point shapes (thin slabs, 3 slices; 7 slots, so the 25- and 9-probe
     rasters leave part-filled groups and mix): each raster matches its own
-    msf_run, and the uniform steps give the same bits as slot passes only."""
+    msf_run, and the grouped steps give the same bits as slot passes only."""
     js = [LargeJob(1024, 6.0, 71, 5), LargeJob(2048, 6.0, 72, 3),
           LargeJob(1024, 6.0, 73, 3), LargeJob(2048, 6.0, 74, 3)]
     ctx = msf.Context(precision="fp32", batch=8)
@@ -121,7 +121,7 @@ def test_large_grid_lanes_match_single_runs(monkeypatch):
     for k, (o, r) in enumerate(zip(outs, singles)):
         assert o.probe_slices == r.probe_slices
         assert_same_run(o, r, 1e-6, 1e-9, "large job %d" % k)
-    monkeypatch.setenv("MSF_LANE_UNIFORM", "0")
+    monkeypatch.setenv("MSF_LANE_GROUPS", "0")
     slot_only = ctx.run_batch(batch, slots=7)
     for k, (a, b) in enumerate(zip(outs, slot_only)):
         assert np.array_equal(a.adf_image, b.adf_image), k
