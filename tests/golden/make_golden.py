@@ -88,6 +88,12 @@ CASES = {
               "-m 2048 2048 300000 --adfstemuncorrfem --V_omega --V_re --cs3 1.3e7 "
               "--scherzer_defocus --scherzer_alphamax --rasterspacing 66 --minslice 2.0 "
               "--images", False, None),
+    # the largest grid the library supports, 4096^2 (a dilute 4 A slab keeps
+    # the reference's atom-by-pixel potential sum short), 300 kV Scherzer
+    "g4096": (dict(n=60, box=(400, 400, 4), seed=81, gen="msf"),
+              "-m 4096 4096 300000 --adfstemuncorrfem --V_omega --cs3 1.3e7 "
+              "--scherzer_defocus --scherzer_alphamax --rasterspacing 200 --minslice 2.0 "
+              "--images", False, None),
     # the precision-stress specimen itself (600k Si, 200x200x300 A, 2048^2,
     # 300 kV, ~150 slices) on a 4x4 raster
     "c4_r4": (dict(n=600000, box=(200, 200, 300), seed=4, gen="msf"),
@@ -119,7 +125,7 @@ CASES = {
 
 # cases whose --images diffraction TIFFs are not kept in the fixture (large
 # grids: only the ADF image and V(k) are compared)
-NO_DIFFRACTION = {"g512", "g2048", "c4_r4"}
+NO_DIFFRACTION = {"g512", "g2048", "g4096", "c4_r4"}
 
 # extra input files of a case, written beside the specimen (name -> text)
 FILES = {
