@@ -77,6 +77,21 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def ncu_l2_bytes(which, nb, pipe):
+    """L2 bytes (lts__t_bytes) per launch of the row or column pass captured
+    at nb probes per launch with the slice-pass variants `pipe`, from the
+    committed ncu summaries; (bytes, file) or (None, None)."""
+    key = "l2_bytes_per_launch_%s_b%d_pipe%s:" % (which, nb, pipe)
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        for line in p.read_text().splitlines():
+            if line.startswith(key):
+                try:
+                    return float(line.split(":", 1)[1].split()[0]), p.name
+                except ValueError:
+                    pass
+    return None, None
+
+
 def ncu_traffic(which, nb, pipe=None):
     """DRAM bytes per launch of the row or column pass ("row" / "col") at nb
     probes per launch, from the committed ncu summaries (profiles/*.md): a
@@ -691,6 +706,13 @@ def main():
     sm_max = clocks.summary().get("sm_max_mhz") or 1965.0
     fp32_peak = fp32_peak_tflops(local, sm_max)
     flop_rate = value / world * flops_ps / 1e12
+    # L2 bytes of the same launch (ncu lts__t_bytes at this tiling): the
+    # L2 rate it implies beside the DRAM one (no measured L2 peak exists
+    # for this part, so no fraction is given)
+    l2_bytes, l2_src = (ncu_l2_bytes(dom, nb, pipe_used)
+                        if (n == 1024 and args.precision == "fp32") else (None, None))
+    l2 = ({"bytes_per_launch": l2_bytes, "achieved_gbs": round(l2_bytes / t_dom / 1e9, 1),
+           "peak": None, "source": l2_src} if l2_bytes else None)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "flops_per_probe_slice": flops_ps,
@@ -701,7 +723,7 @@ def main():
                           (dom, "transmission" if dom == "row" else "propagator", nb),
                 "peak_source": peak_kind, "ms_row": round(ms_row, 4), "ms_col": round(ms_col, 4),
                 "algorithmic_bytes_per_launch": alg, "live_column_fraction": round(live, 4),
-                "traffic_source": traffic_src,
+                "traffic_source": traffic_src, "l2": l2,
                 "timing": timing}
 
     # end to end through the C ABI from host buffers
