@@ -626,14 +626,17 @@ cudaError_t launch_col_slice_pipe(const PassArgs& a, bool last, const void* tens
 // 8-byte elements (one per FP32 complex value, two per FP64 one), box
 // {cols, min(256, nx)} rows; no multicast, no swizzle.
 cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out, bool fp64) {
-  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  if (!encode) {
+  // looked up once per process (a thread-safe static: lanes of the request
+  // loop encode maps from their worker thread)
+  static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
     cudaDriverEntryPointQueryResult q;
     void* fn = nullptr;
     cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
-    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  }
+    return (e == cudaSuccess && q == cudaDriverEntryPointSuccess)
+               ? reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn)
+               : nullptr;
+  }();
+  if (!encode) return cudaErrorNotSupported;
   const int cols = pipe_cols_for(nx, fp64);
   if (!cols) return cudaErrorInvalidValue;
   const int epc = fp64 ? 2 : 1;  // 8-byte elements per complex value
