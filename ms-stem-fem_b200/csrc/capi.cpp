@@ -107,6 +107,10 @@ msf_status msf_context_destroy(msf_context* ctx) {
     ctx->pool->closed = true;
   }
   ctx->pool->trim();
+  if (ctx->host_stage) {
+    std::lock_guard<std::recursive_mutex> cap(msf::capture_mutex());
+    cudaFreeHost(ctx->host_stage);
+  }
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return MSF_OK;

@@ -912,20 +912,31 @@ msf_status download_sums(msf_context* ctx, const RasterPlan& P, cudaStream_t str
 msf_status finish_raster(msf_context* ctx, const RasterPlan& P, cudaStream_t stream,
                          msf_results* res) {
   TraceScope trace_scope("raster_finish");
-  std::vector<double> amp((size_t)P.n_probes * P.n_seg), inten((size_t)P.n_probes * P.n_seg);
-  std::vector<double> acc_a, acc_i;
-  if (P.pix_modes) {
-    acc_a.resize(P.plane);
-    acc_i.resize(P.plane);
+  // the sums land in the context's pinned staging buffer (no page faults on
+  // fresh host memory, copies at the pinned rate)
+  const size_t rows = (size_t)P.n_probes * P.n_seg;
+  const size_t pix = P.pix_modes ? (size_t)P.plane : 0;
+  const size_t need = sizeof(double) * (2 * rows + 2 * pix);
+  std::lock_guard<std::mutex> lock(ctx->stage_mu);
+  if (ctx->host_stage_bytes < need) {
+    // freeing pinned memory can wait on the device: not during a capture
+    // on another thread
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
+    if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+    ctx->host_stage = nullptr;
+    ctx->host_stage_bytes = 0;
+    MSF_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ctx->host_stage), need,
+                           cudaHostAllocDefault));
+    ctx->host_stage_bytes = need;
   }
-  MSF_TRY(download_sums(ctx, P, stream, amp.data(), inten.data(),
-                        P.pix_modes ? acc_a.data() : nullptr,
-                        P.pix_modes ? acc_i.data() : nullptr));
+  double* amp = ctx->host_stage;
+  double* inten = amp + rows;
+  double* acc_a = P.pix_modes ? inten + rows : nullptr;
+  double* acc_i = P.pix_modes ? acc_a + pix : nullptr;
+  MSF_TRY(download_sums(ctx, P, stream, amp, inten, acc_a, acc_i));
   static const Rings no_rings;
   return finish_host(P.spec->g, P.rings ? *P.rings : no_rings, P.optics, P.det, P.n_probes,
-                     amp.data(),
-                     inten.data(), P.pix_modes ? acc_a.data() : nullptr,
-                     P.pix_modes ? acc_i.data() : nullptr, res);
+                     amp, inten, acc_a, acc_i, res);
 }
 
 msf_status finish_host(const Grid& g, const Rings& rings, const msf_optics& optics,

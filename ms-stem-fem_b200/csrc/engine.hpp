@@ -138,6 +138,12 @@ struct msf_context {
   };
   std::map<RingKey, std::shared_ptr<const msf::Rings>> ring_cache;
   std::mutex ring_mu;
+  // pinned host buffer the per-probe and per-pixel sums of a raster are
+  // copied into before the host finish (grown on demand, reused by every
+  // raster; freed with the context)
+  double* host_stage = nullptr;
+  size_t host_stage_bytes = 0;
+  std::mutex stage_mu;
   // specimens built by this context keep a host copy of every slice's
   // projected potential before the exponential (msf_specimen_potential)
   bool keep_potentials = false;
