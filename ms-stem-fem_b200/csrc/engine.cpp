@@ -151,7 +151,10 @@ msf_status msf_context::twiddles(int n, bool want64, const void** out) {
   auto it = m.find(n);
   if (it == m.end()) {
     std::vector<double> h(2 * (size_t)n);
-    fill_twiddles(n, h.data());
+    if (want64)
+      fill_twiddles(n, h.data());
+    else  // the FP32 passes also read each stage's factors as [r][k] copies
+      fill_twiddles_f32_table(n, h);
     DevBuf b;
     if (want64) {
       MSF_TRY(upload(this, &b, h));

@@ -216,6 +216,11 @@ template <int N, typename Real, int V = 0> struct Shape;
     __host__ __device__ static constexpr int ns(int s) {                                          \
       return s == 0 ? 1 : s == 1 ? R0 : R0 * R1;                              \
     }                                                                         \
+    /* stage twiddles also stored as [r][k] after the N-entry table */        \
+    static constexpr bool TT = sizeof(REAL_) == 4 && V_ == 0;                 \
+    __host__ __device__ static constexpr int tt_off(int s) {                  \
+      return s <= 1 ? 0 : tt_off(s - 1) + (radix(s - 1) - 1) * ns(s - 1);     \
+    }                                                                         \
   };
 MSF_SHAPE(64, float, 0, 8, 2, 8, 8, 1)
 MSF_SHAPE(128, float, 0, 16, 2, 16, 8, 1)
@@ -298,8 +303,11 @@ struct Smem {
 
 // Transform one line in place.  v[m] holds element t + T*m on entry and
 // X[t + T*m] on exit.  `sm` is this line's shared buffer (Smem<Sh>::stride
-// elements), `tw` the table e^{-2 pi i m / N}, m < N, and `sync` a barrier
-// over all threads that share `sm` lines with this one.
+// elements), `tw` the table e^{-2 pi i m / N}, m < N (for Sh::TT shapes
+// followed by each stage s >= 1's factors e^{-2 pi i r k / (NS R)} as
+// [r - 1][k], r < R, k < NS, at N + Sh::tt_off(s): copies of table entries,
+// laid out so that a warp's lanes read consecutive addresses), and `sync` a
+// barrier over all threads that share `sm` lines with this one.
 template <class Sh, bool INV, typename C, class Sync>
 __device__ __forceinline__ void fft_line(C (&v)[Sh::E], C* __restrict__ sm,
                                          int t, const C* __restrict__ tw,
@@ -331,7 +339,10 @@ __device__ __forceinline__ void fft_line(C (&v)[Sh::E], C* __restrict__ sm,
           // keep at most kLoadChunk table loads in flight: bounds the
           // registers the compiler spends on hoisted twiddles
           if constexpr (r % kLoadChunk == 0) load_fence();
-          const C w = __ldg(&tw[r * k * (N / (NS * R))]);
+          // Sh::TT: the same value from the stage's [r][k] copy, so that
+          // the lanes of a warp (consecutive k) read consecutive entries
+          const C w = Sh::TT ? __ldg(&tw[N + Sh::tt_off(s) + (r - 1) * NS + k])
+                             : __ldg(&tw[r * k * (N / (NS * R))]);
           v[b + r * NB] = INV ? cmulc(v[b + r * NB], w) : cmul(v[b + r * NB], w);
         });
       }

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 
 namespace msf {
 
@@ -1122,6 +1123,40 @@ void fill_twiddles(int n, double* h) {
     const double a = two_pi * (double)m / (double)n;
     h[2 * m] = std::cos(a);
     h[2 * m + 1] = -std::sin(a);
+  }
+}
+
+namespace {
+template <int N>
+void append_stage_twiddles(const double* base, std::vector<double>& out) {
+  using Sh = Shape<N, float, 0>;
+  static_assert(Sh::TT, "stage copies are laid out for the FP32 main schedule");
+  for (int s = 1; s < Sh::S; ++s) {
+    const int R = Sh::radix(s), NS = Sh::ns(s);
+    if ((int)out.size() != 2 * (N + Sh::tt_off(s))) std::abort();  // layout drift
+    for (int r = 1; r < R; ++r)
+      for (int k = 0; k < NS; ++k) {
+        const int m = r * k * (N / (NS * R));
+        out.push_back(base[2 * m]);
+        out.push_back(base[2 * m + 1]);
+      }
+  }
+}
+}  // namespace
+
+void fill_twiddles_f32_table(int n, std::vector<double>& h) {
+  h.assign(2 * (size_t)n, 0.0);
+  fill_twiddles(n, h.data());
+  const std::vector<double> base = h;
+  switch (n) {
+    case 64: append_stage_twiddles<64>(base.data(), h); break;
+    case 128: append_stage_twiddles<128>(base.data(), h); break;
+    case 256: append_stage_twiddles<256>(base.data(), h); break;
+    case 512: append_stage_twiddles<512>(base.data(), h); break;
+    case 1024: append_stage_twiddles<1024>(base.data(), h); break;
+    case 2048: append_stage_twiddles<2048>(base.data(), h); break;
+    case 4096: append_stage_twiddles<4096>(base.data(), h); break;
+    default: break;  // no FP32 pass of this length
   }
 }
 
