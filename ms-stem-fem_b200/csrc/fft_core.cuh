@@ -216,8 +216,10 @@ template <int N, typename Real, int V = 0> struct Shape;
     __host__ __device__ static constexpr int ns(int s) {                                          \
       return s == 0 ? 1 : s == 1 ? R0 : R0 * R1;                              \
     }                                                                         \
+    using Real = REAL_;                                                       \
+    static constexpr int V = V_;                                              \
     /* stage twiddles also stored as [r][k] after the N-entry table */        \
-    static constexpr bool TT = sizeof(REAL_) == 4 && V_ == 0;                 \
+    static constexpr bool TT = sizeof(REAL_) == 4;                            \
     __host__ __device__ static constexpr int tt_off(int s) {                  \
       return s <= 1 ? 0 : tt_off(s - 1) + (radix(s - 1) - 1) * ns(s - 1);     \
     }                                                                         \
@@ -241,6 +243,19 @@ MSF_SHAPE(1024, double, 0, 16, 3, 16, 16, 4)
 MSF_SHAPE(2048, double, 0, 16, 3, 16, 16, 8)
 MSF_SHAPE(4096, double, 0, 16, 3, 16, 16, 16)
 #undef MSF_SHAPE
+
+// Where a TT shape's stage copies start in the FP32 table: after the N plain
+// entries for the main schedule (V = 0), after those and the main
+// schedule's copies for the alternative one (V = 1).
+template <class Sh>
+__host__ __device__ constexpr int tt_base() {
+  if constexpr (Sh::V == 0) {
+    return Sh::N;
+  } else {
+    using S0 = Shape<Sh::N, typename Sh::Real, 0>;
+    return S0::N + S0::tt_off(S0::S);
+  }
+}
 
 // Worst bank multiplicity of one shared-memory access phase (128 bytes of
 // lanes) over the exchanges of a line FFT, for lines `stride` elements
@@ -305,7 +320,7 @@ struct Smem {
 // X[t + T*m] on exit.  `sm` is this line's shared buffer (Smem<Sh>::stride
 // elements), `tw` the table e^{-2 pi i m / N}, m < N (for Sh::TT shapes
 // followed by each stage s >= 1's factors e^{-2 pi i r k / (NS R)} as
-// [r - 1][k], r < R, k < NS, at N + Sh::tt_off(s): copies of table entries,
+// [r - 1][k], r < R, k < NS, at tt_base<Sh>() + Sh::tt_off(s): copies of table entries,
 // laid out so that a warp's lanes read consecutive addresses), and `sync` a
 // barrier over all threads that share `sm` lines with this one.
 template <class Sh, bool INV, typename C, class Sync>
@@ -341,7 +356,7 @@ __device__ __forceinline__ void fft_line(C (&v)[Sh::E], C* __restrict__ sm,
           if constexpr (r % kLoadChunk == 0) load_fence();
           // Sh::TT: the same value from the stage's [r][k] copy, so that
           // the lanes of a warp (consecutive k) read consecutive entries
-          const C w = Sh::TT ? __ldg(&tw[N + Sh::tt_off(s) + (r - 1) * NS + k])
+          const C w = Sh::TT ? __ldg(&tw[tt_base<Sh>() + Sh::tt_off(s) + (r - 1) * NS + k])
                              : __ldg(&tw[r * k * (N / (NS * R))]);
           v[b + r * NB] = INV ? cmulc(v[b + r * NB], w) : cmul(v[b + r * NB], w);
         });

@@ -1127,13 +1127,13 @@ void fill_twiddles(int n, double* h) {
 }
 
 namespace {
-template <int N>
+template <int N, int V = 0>
 void append_stage_twiddles(const double* base, std::vector<double>& out) {
-  using Sh = Shape<N, float, 0>;
-  static_assert(Sh::TT, "stage copies are laid out for the FP32 main schedule");
+  using Sh = Shape<N, float, V>;
+  static_assert(Sh::TT, "stage copies are laid out for the FP32 schedules");
   for (int s = 1; s < Sh::S; ++s) {
     const int R = Sh::radix(s), NS = Sh::ns(s);
-    if ((int)out.size() != 2 * (N + Sh::tt_off(s))) std::abort();  // layout drift
+    if ((int)out.size() != 2 * (tt_base<Sh>() + Sh::tt_off(s))) std::abort();  // layout drift
     for (int r = 1; r < R; ++r)
       for (int k = 0; k < NS; ++k) {
         const int m = r * k * (N / (NS * R));
@@ -1151,10 +1151,22 @@ void fill_twiddles_f32_table(int n, std::vector<double>& h) {
   switch (n) {
     case 64: append_stage_twiddles<64>(base.data(), h); break;
     case 128: append_stage_twiddles<128>(base.data(), h); break;
-    case 256: append_stage_twiddles<256>(base.data(), h); break;
-    case 512: append_stage_twiddles<512>(base.data(), h); break;
-    case 1024: append_stage_twiddles<1024>(base.data(), h); break;
-    case 2048: append_stage_twiddles<2048>(base.data(), h); break;
+    case 256:
+      append_stage_twiddles<256>(base.data(), h);
+      append_stage_twiddles<256, 1>(base.data(), h);
+      break;
+    case 512:
+      append_stage_twiddles<512>(base.data(), h);
+      append_stage_twiddles<512, 1>(base.data(), h);
+      break;
+    case 1024:
+      append_stage_twiddles<1024>(base.data(), h);
+      append_stage_twiddles<1024, 1>(base.data(), h);
+      break;
+    case 2048:
+      append_stage_twiddles<2048>(base.data(), h);
+      append_stage_twiddles<2048, 1>(base.data(), h);
+      break;
     case 4096: append_stage_twiddles<4096>(base.data(), h); break;
     default: break;  // no FP32 pass of this length
   }

@@ -206,8 +206,8 @@ cudaError_t encode_column_map(void* psi, int nb, int nx, int ny, void* map_out,
 // Twiddle table e^{-2 pi i m / n}, m < n, computed in FP64 on the host.
 void fill_twiddles(int n, double* host_interleaved /* 2n */);
 // The FP32 passes' table: fill_twiddles' n entries followed by each stage's
-// factors again as [r][k] (copies of table entries, in the order the main
-// FP32 schedule of length n reads them).
+// factors again as [r][k] (copies of table entries, in the order the FP32
+// schedules of length n read them: the main one, then the alternative).
 void fill_twiddles_f32_table(int n, std::vector<double>& host_interleaved);
 
 // ---- set-up kernels (FP64) ----
