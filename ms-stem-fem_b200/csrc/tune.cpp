@@ -65,6 +65,7 @@ msf_status tune(msf_context* ctx, const msf_specimen* spec, msf_tuning* out) {
               MSF_ROW_PREFETCH | MSF_ROW_BYPROBE,
               MSF_ROW_PREFETCH | MSF_ROW_L2AHEAD | MSF_ROW_BYPROBE,
               MSF_ROW_ALT,
+              MSF_ROW_PREFETCH | MSF_ROW_ALT,
               MSF_ROW_STAGED,
               MSF_ROW_STAGED | MSF_ROW_ALT};
     pipes.clear();

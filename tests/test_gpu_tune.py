@@ -23,7 +23,7 @@ def test_tune_picks_a_candidate_and_keeps_results(precision):
     t = ctx.tune(spec)
     assert (t["nx"], t["ny"]) == (256, 256)
     assert t["batch"] in (8, 16, 32, 64, 128, 256)
-    fp32_pipes = (0, 1, 4, 5, 8, 9, 12, 13, 16, 17, 32, 33, 48, 49, 80, 81, 112, 113)
+    fp32_pipes = (0, 1, 4, 5, 8, 9, 12, 13, 16, 17, 24, 25, 32, 33, 48, 49, 80, 81, 112, 113)
     assert t["pipe"] in (fp32_pipes if precision == "fp32" else (0, 1))
     assert t["ns_per_probe_slice"] > 0
     after = ctx.run(spec, j.optics, j.raster, j.detect)
